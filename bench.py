@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the XPBD substep engine on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload spheres|cloth]
+    python bench.py --impl reference ...      # the CPU restatement of the reference, timed on the host
+
+A step is one frame (dt = 1/60 s, 15 substeps x 2 iterations) of the workload.
+Default workload: the 2048-sphere pile (16 x 8 x 16 jittered lattice, r = 0.05 m,
+FLOOR rows, sphere-sphere self collision regenerated every frame, Jacobi).  The
+metric is constraint projections per second (rows x substeps x iterations per
+frame, the reference's benchmark definition, examples/benchmark.py:126) and
+ms/frame.  Multi-GPU runs are independent replicas (one scene per rank, no data
+exchange): value = sum over ranks of projections / max over ranks of time.
+
+Timing: W untimed frames, then K frames each bracketed by CUDA events on the
+solver's stream, with the 126 MB L2 flushed (256 MB memset) between frames
+outside the events; barrier + synchronize on both sides; max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "spheres": "sphere pile 2048 (16x8x16, r=0.05 m, jitter 0.01, floor + self collision mu=0.5), jacobi 15x2",
+    "cloth": "cloth 32x32 (spacing 0.02 m, 0.01 kg, 2 pinned corners, 5826 DISTANCE alpha=1e-8 + 1024 FLOOR mu=0.3), gs 15x2",
+    "cloth_jacobi": "cloth 32x32 as above, jacobi 15x2",
+}
+BYTES_PER_PROJ = {0: 88, 1: 88, 2: 64, 3: 112}   # DISTANCE, ATTACH, FLOOR, CONTACT (Jacobi)
+BYTES_PER_PROJ_GS = {0: 84, 1: 84, 2: 64, 3: 112}
+APPLY_BYTES = 60          # per body per iteration (Jacobi averaged apply)
+BODY_SUBSTEP_BYTES = 128  # per body per substep (integrate + finalize + clamp)
+
+
+def make_solver(workload, device, solver_cls):
+    from xpbd_b200 import scenes
+    if workload == "spheres":
+        s = solver_cls(dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi", device=device)
+        scenes.build_sphere_pile(s)
+    elif workload in ("cloth", "cloth_jacobi"):
+        mode = "gs" if workload == "cloth" else "jacobi"
+        s = solver_cls(dt=1 / 60, substeps=15, iterations=2, solve_mode=mode, device=device)
+        scenes.build_cloth(s)
+    else:
+        raise SystemExit(f"unknown workload {workload}")
+    return s
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_for(workload):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(workload)
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.seek(0)
+        rows = [r.split(", ") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) >= 9:
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip() == "Active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(solver, rows_type_counts, gs):
+    S, I, n = solver.substeps, solver.iterations, solver.num_bodies
+    table = BYTES_PER_PROJ_GS if gs else BYTES_PER_PROJ
+    b = S * I * sum(table[t] * c for t, c in rows_type_counts.items())
+    if not gs:
+        b += S * I * n * APPLY_BYTES
+    b += S * n * BODY_SUBSTEP_BYTES
+    return b
+
+
+def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from xpbd_b200 import Solver
+    from xpbd_b200 import _native as N
+
+    s = make_solver(workload, device, Solver)
+    s.sync_contacts = False  # contact-capacity overflow is checked once after the run
+    gs = s.solve_mode == "gs"
+    L = N.lib()
+    stream = torch.cuda.current_stream(device)
+    sp = C.c_void_p(stream.cuda_stream)
+    launches_per_frame = 1 + (10 if s._self_collision else 0)
+
+    def frame():
+        if s._self_collision:
+            s._build_contacts(sp)
+        N.check(L.xpbd3_step(s._h, 1, sp), "xpbd3_step")
+
+    s._flush()
+    for _ in range(args.warmup):
+        frame()
+    torch.cuda.synchronize(device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    rows_total = 0
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
+        for k in range(args.steps):
+            if flush_buf is not None:
+                flush_buf.zero_()
+            e0, e1, e2 = ev[k]
+            e0.record(stream)
+            if s._self_collision:
+                s._build_contacts(sp)
+            e1.record(stream)
+            N.check(L.xpbd3_step(s._h, 1, sp), "xpbd3_step")
+            e2.record(stream)
+        torch.cuda.synchronize(device)
+    frame_ms = [a.elapsed_time(c) for a, _, c in ev]
+    kern_ms = [b.elapsed_time(c) for _, b, c in ev]
+    status = s.status()
+    rows = s.rows()
+    types, counts = np.unique(rows["type"], return_counts=True)
+    type_counts = {int(t): int(c) for t, c in zip(types, counts)}
+    m = int(len(rows["type"]))
+    proj_per_frame = m * s.substeps * s.iterations
+    total_ms = sum(frame_ms)
+    alg_bytes = algorithmic_bytes(s, type_counts, gs)
+    res = dict(total_ms=total_ms, frame_ms=frame_ms, kern_ms=kern_ms, proj_per_frame=proj_per_frame,
+               rows=m, bodies=s.num_bodies, status=status, alg_bytes=alg_bytes,
+               launches=launches_per_frame * args.steps, solver=s)
+    blocks, threads, smem = C.c_int(), C.c_int(), C.c_int()
+    L.xpbd3_launch_info(s._h, C.byref(blocks), C.byref(threads), C.byref(smem))
+    res["launch"] = dict(blocks=blocks.value, threads=threads.value, smem_bytes=smem.value)
+    return res
+
+
+def time_e2e(args, workload, device):
+    """Same metric through the public API with host buffers: each frame uploads
+    the particle state from pinned host memory, steps, and reads the positions
+    back into pinned host memory, all inside the CUDA-event-timed region."""
+    import torch
+
+    from xpbd_b200 import Solver
+    s = make_solver(workload, device, Solver)
+    s.sync_contacts = False
+    s._flush()
+    T = s.tensors
+    hx = T["x"].cpu().pin_memory()
+    hv = T["v"].cpu().pin_memory()
+    out = torch.empty_like(hx).pin_memory()
+    stream = torch.cuda.current_stream(device)
+    for _ in range(max(3, args.warmup // 2)):
+        T["x"].copy_(hx, non_blocking=True); T["v"].copy_(hv, non_blocking=True)
+        s.step()
+        out.copy_(T["x"], non_blocking=True)
+        hx.copy_(out)
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    steps = max(1, args.steps // 2)
+    e0.record(stream)
+    for _ in range(steps):
+        T["x"].copy_(hx, non_blocking=True)
+        T["v"].copy_(hv, non_blocking=True)
+        s.step()
+        out.copy_(T["x"], non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1) / steps
+    m = s.num_constraints
+    h2d = hx.numel() * 4 + hv.numel() * 4
+    d2h = out.numel() * 4
+    return ms, m * s.substeps * s.iterations, h2d, d2h
+
+
+def cpu_baseline(workload, seconds):
+    """The oracle (CPU restatement of the reference) on a bounded sample of the
+    same workload: consecutive frames from the same initial state until
+    `seconds` of host time have elapsed (at least one frame)."""
+    from oracle import oracle as O
+    s = make_solver(workload, "cpu", O.OracleSolver)
+    s.step()  # first frame outside the sample (builds arrays)
+    t0 = time.perf_counter()
+    frames = 0
+    proj = 0
+    while True:
+        s.step()
+        frames += 1
+        proj += s.num_constraints * s.substeps * s.iterations
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return proj / dt / 1e6, frames, dt
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    t0 = time.perf_counter()
+    from oracle import oracle as O
+    s = make_solver(args.workload, "cpu", O.OracleSolver)
+    for _ in range(args.warmup):
+        s.step()
+    times = []
+    proj = 0
+    for _ in range(args.steps):
+        a = time.perf_counter()
+        s.step()
+        times.append(time.perf_counter() - a)
+        proj += s.num_constraints * s.substeps * s.iterations
+    total = sum(times)
+    value = proj / total / 1e6
+    line = {
+        "impl": "reference", "metric": "constraint projections per second", "value": round(value, 4),
+        "unit": "M proj/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total / args.steps * 1e3, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOADS[args.workload], "frames_per_step": 1},
+        "cpu_baseline": {"value": round(value, 4), "unit": "M proj/s", "cores": 1, "kind": "port",
+                         "sample": f"{args.steps} consecutive frames after {args.warmup} warm-up frames"},
+        "e2e": {"value": round(value, 4), "unit": "M proj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(time.perf_counter() - t0, 2),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="spheres", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-flush", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(device))
+    flush = None if args.no_flush else torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    clocks = Clocks(local)
+    r = time_engine(args, args.workload, device, rank, world, flush, clocks)
+    total_ms = r["total_ms"]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * r["proj_per_frame"] * args.steps / (total_ms / 1e3) / 1e6
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        kern_ms = statistics.mean(r["kern_ms"])
+        achieved = r["alg_bytes"] / (kern_ms / 1e3) / 1e9
+        line = {
+            "metric": "constraint projections per second", "value": round(value, 4), "unit": "M proj/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded numpy default_rng(0))",
+            "config": {"workload": WORKLOADS[args.workload], "bodies": r["bodies"], "rows_last_frame": r["rows"],
+                       "frames_per_step": 1, "l2": "flushed between frames (256 MB memset outside the timed events)",
+                       "parallelism": f"replicas x{world}", "launch": r["launch"]},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 5), "peak_kind": peak_kind,
+                         "traffic": traffic_for(args.workload), "kernel": "k3_frames (persistent frame kernel)",
+                         "kernel_ms": round(kern_ms, 5), "alg_bytes_per_launch": r["alg_bytes"]},
+            "gpu_launches": r["launches"],
+            "status_bits": r["status"],
+        }
+        line["clocks"] = clocks.summary()
+        try:
+            e_ms, e_proj, h2d, d2h = time_e2e(args, args.workload, device)
+            line["e2e"] = {"value": round(world * e_proj / (e_ms / 1e3) / 1e6, 4), "unit": "M proj/s",
+                           "ms_per_step": round(e_ms, 5), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        except Exception as e:  # pragma: no cover - reported, never silent
+            line["e2e"] = {"error": repr(e)}
+        if world == 1:
+            v, frames, secs = cpu_baseline(args.workload, args.cpu_seconds)
+            line["cpu_baseline"] = {"value": round(v, 4), "unit": "M proj/s", "cores": 1, "kind": "port",
+                                    "sample": f"{frames} consecutive frames of the same workload ({secs:.1f} s)"}
+            if not args.no_extras:
+                extras = {}
+                for wl in WORKLOADS:
+                    if wl == args.workload:
+                        continue
+                    a2 = argparse.Namespace(**vars(args))
+                    a2.steps = min(args.steps, 50)
+                    rr = time_engine(a2, wl, device, 0, 1, flush, None)
+                    ms = rr["total_ms"] / a2.steps
+                    extras[wl] = {"ms_per_frame": round(ms, 5),
+                                  "M_proj_per_s": round(rr["proj_per_frame"] / (ms / 1e3) / 1e6, 3),
+                                  "kernel_ms": round(statistics.mean(rr["kern_ms"]), 5), "launch": rr["launch"]}
+                line["other_workloads"] = extras
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,215 @@
+/*
+ * xpbd_b200.h -- C ABI of the B200 XPBD substep engine (libxpbd_b200.so).
+ *
+ * The reference (nanli9/XPBD, package xpbd3d) has no native interface: its hot
+ * path is a set of Warp kernels launched from Python.  Each entry point below
+ * replaces one of those kernels or host routines; the reference function is
+ * cited beside it (paths relative to the reference project).
+ *
+ * Conventions
+ *  - Every call returns an int status: XPBD_OK or an XPBD_ERR_* code.
+ *  - Device pointers are plain `float*` / `int*`; the caller owns all state
+ *    memory.  Layouts are fixed-width records:
+ *        "float4" = 4 consecutive floats, 16-byte aligned,
+ *        "int4"   = 4 consecutive int32, 16-byte aligned,
+ *        "int2"   = 2 consecutive int32, 8-byte aligned.
+ *  - `stream` is a cudaStream_t passed as void*; NULL is the legacy stream.
+ *    Every device entry point is asynchronous on that stream.
+ *  - All arithmetic is fp32.
+ *  - A solver handle is not thread safe; use one handle per stream.
+ */
+#ifndef XPBD_B200_H
+#define XPBD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status -------------------------------------------------------------- */
+#define XPBD_OK 0
+#define XPBD_ERR_BAD_ARG 1
+#define XPBD_ERR_CUDA 2
+/* bits of the device status word (xpbd*_status) */
+#define XPBD_ERR_OVERFLOW 4          /* a fixed-capacity buffer (pairs, contacts) overflowed */
+#define XPBD_ERR_NAN 8               /* a non-finite position was seen and reset */
+#define XPBD_ERR_BARRIER_TIMEOUT 16  /* a persistent kernel's grid barrier gave up waiting */
+#define XPBD_ERR_BAD_INDEX 32        /* a row or pair referenced a body out of range */
+
+/* constraint row types (kernels.py:36-40) */
+#define XPBD_DISTANCE 0
+#define XPBD_ATTACH 1
+#define XPBD_FLOOR 2
+#define XPBD_CONTACT 3
+
+const char* xpbd_version(void);
+/* Last CUDA error string recorded by a call that returned XPBD_ERR_CUDA. */
+const char* xpbd_last_error(void);
+
+/* ========================================================================== */
+/* 3-DOF particle solver (replaces solver.py:57-508 + kernels.py)              */
+/* ========================================================================== */
+typedef struct xpbd3_state {
+    int n_bodies;            /* particles                                      */
+    int row_capacity;        /* rows allocated (static rows + contact capacity) */
+    int n_rows_static;       /* rows that are not generated contacts           */
+    float* x;                /* float4[n]: position xyz, inverse mass w        */
+    float* v;                /* float4[n]: velocity xyz, w unused              */
+    float* x_prev;           /* float4[n]: substep-start position, w unused    */
+    float* acc;              /* float4[n]: Jacobi accumulator dx xyz, count w (zero between calls) */
+    int* row_i;              /* int4[cap]: type, body a, body b, active        */
+    float* row_f;            /* float4[cap]: rest, compliance, mu, floor y     */
+    float* row_anchor;       /* float4[cap]: ATTACH world anchor xyz           */
+    float* lam;              /* float[cap]: multipliers                        */
+    int* n_rows;             /* int[1] on device: live row count (static + contacts) */
+    const int* color_order;  /* int[cap]: rows sorted by color (GS)            */
+    const int* color_starts; /* int[num_colors+1] on device (GS)               */
+    int num_colors;
+} xpbd3_state;
+
+typedef struct xpbd3_params {
+    double dt;               /* frame time step (s)                            */
+    int substeps, iterations;
+    float gravity[3];
+    float damping, jacobi_relax;
+    float max_speed;         /* <= 0 or inf disables the clamp                 */
+    int gs;                  /* 1: colored Gauss-Seidel, 0: Jacobi             */
+} xpbd3_params;
+
+/* kernels.py:49-73 integrate */
+int xpbd3_integrate(const xpbd3_state* s, float h, float gx, float gy, float gz, void* stream);
+/* kernels.py:219-322 solve_constraints_jacobi; first != 0 treats lambda as the
+ * substep's freshly zeroed multipliers (solver.py:430-431). */
+int xpbd3_solve_jacobi(const xpbd3_state* s, float h, int first, void* stream);
+/* kernels.py:326-339 apply_jacobi */
+int xpbd3_apply_jacobi(const xpbd3_state* s, float relax, void* stream);
+/* kernels.py:105-208 solve_constraints_color over color_order[start, start+count) */
+int xpbd3_solve_color(const xpbd3_state* s, int start, int count, float h, int first, void* stream);
+/* kernels.py:346-358 finalize_velocity */
+int xpbd3_finalize_velocity(const xpbd3_state* s, float h, float damping, void* stream);
+/* kernels.py:362-371 cap_velocity */
+int xpbd3_cap_velocity(const xpbd3_state* s, float max_speed, void* stream);
+
+/* solver.py:412-442 Solver.step substep loop.  A solver handle runs whole
+ * frames in one persistent launch per frame (or per `frames` batch), captured
+ * in a CUDA graph. */
+typedef struct xpbd3_solver xpbd3_solver;
+int xpbd3_create(xpbd3_solver** out);
+int xpbd3_destroy(xpbd3_solver* h);
+int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_params* p);
+int xpbd3_step(xpbd3_solver* h, int frames, void* stream);
+/* Copies the device status word (XPBD_ERR_* bits) to *out and clears it. */
+int xpbd3_status(xpbd3_solver* h, int* out, void* stream);
+/* Launch configuration chosen by the last bind: blocks, threads, shared bytes. */
+int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int* smem_bytes);
+
+/* coloring.py:26-71 color_constraints (host, Welsh-Powell, bit-exact order).
+ * Returns the number of colors, or -1 on bad arguments. */
+int xpbd_color_constraints(int n_bodies, int m, const int* a, const int* b, int* color);
+/* coloring.py:74-89 color_ranges (host). starts has num_colors+1 entries. */
+int xpbd_color_ranges(int m, const int* color, int* order, int* starts);
+
+/* solver.py:275-342 _rebuild_contacts + solver.py:469-483 _sanitize_positions,
+ * on the device.  Resets non-finite positions to x_init (float4[n]) with zero
+ * velocity, then regenerates the CONTACT rows at [n_rows_static, row_capacity)
+ * in the reference's order and writes the live row count to s->n_rows.
+ * radius/friction: float[n]; collide_idx: int[n_collide] collidable bodies in
+ * ascending order; existing: sorted int64 keys min*n+max of body pairs already
+ * joined by a two-body row; contact_margin, dt and r_max (largest collidable
+ * radius) are the host's fp64 values.  Overflow of the contact capacity and
+ * reset positions set XPBD_ERR_OVERFLOW / XPBD_ERR_NAN in *status_dev. */
+typedef struct xpbd3_contacts xpbd3_contacts;
+int xpbd3_contacts_create(xpbd3_contacts** out, int n_bodies, int n_collide);
+int xpbd3_contacts_destroy(xpbd3_contacts* c);
+int xpbd3_contacts_build(xpbd3_contacts* c, const xpbd3_state* s, const float* radius,
+                         const float* friction, const int* collide_idx, int n_collide,
+                         const int64_t* existing, int n_existing, const float* x_init,
+                         double contact_margin, double dt, double r_max, int* status_dev,
+                         void* stream);
+
+/* Device primitives exposed for tests (no reference counterpart): stable sort
+ * of uint64 keys with uint32 values, and exclusive scan of int32. */
+int xpbd_sort_pairs_u64(uint64_t* keys, uint32_t* vals, int n, int max_bits, void* stream);
+int xpbd_scan_i32(const int* in, int* out, int n, int* total, void* stream);
+
+/* ========================================================================== */
+/* 6-DOF rigid-body solver (replaces solver_6dof.py:79-559 + kernels_6dof.py,  */
+/* kernels_bvh.py, kernels_hashgrid.py)                                        */
+/* ========================================================================== */
+typedef struct xpbd6_state {
+    int n_bodies, n_joints, pair_capacity;
+    float* x;        /* float4[n]: position xyz, inverse mass w          */
+    float* q;        /* float4[n]: orientation (x, y, z, w)              */
+    float* v;        /* float4[n]: linear velocity                       */
+    float* w;        /* float4[n]: angular velocity (world)              */
+    float* x_prev;   /* float4[n] */
+    float* q_prev;   /* float4[n] */
+    float* inv_I;    /* float4[n]: body-frame diagonal inverse inertia   */
+    float* he;       /* float4[n]: half extents xyz                      */
+    int* group;      /* int[n]: no-self-collision group (> 0)            */
+    float* acc_x;    /* float4[n]: Jacobi dx xyz, count w                */
+    float* acc_r;    /* float4[n]: Jacobi drot xyz                       */
+    float* acc_v;    /* float4[n]: velocity-pass dv xyz, count w         */
+    float* acc_w;    /* float4[n]: velocity-pass dw xyz                  */
+    float* lam_floor;/* float[8n]                                        */
+    int* pairs;      /* int2[cap]: candidate pairs                       */
+    int* n_pairs;    /* int[1] on device                                 */
+    int* m_hdr;      /* int4[cap]: manifold count, incident, reference   */
+    float* m_normal; /* float4[cap]                                      */
+    float* m_off_inc;/* float4[8 cap]                                    */
+    float* m_off_ref;/* float4[8 cap]                                    */
+    float* lam_pair; /* float[8 cap]                                     */
+    int* j_ab;       /* int2[n_joints]                                   */
+    float* j_anchor_a; /* float4[n_joints]: anchor in A's frame, rest w  */
+    float* j_anchor_b; /* float4[n_joints]: anchor in B's frame, compliance w */
+    float* lam_joint;  /* float[n_joints]                                */
+} xpbd6_state;
+
+typedef struct xpbd6_params {
+    double dt;
+    int substeps, iterations, gyroscopic;
+    float gravity[3];
+    float floor_y, friction, restitution, lin_damp, ang_damp, jacobi_relax;
+    float max_speed, max_omega, man_margin;
+    int broadphase;  /* 0 lbvh, 1 hashgrid, 2 grid */
+} xpbd6_params;
+
+/* kernels_6dof.py:68-102 integrate_bodies */
+int xpbd6_integrate(const xpbd6_state* s, const xpbd6_params* p, void* stream);
+/* kernels_6dof.py:234-382 generate_box_manifold over the device pair list */
+int xpbd6_manifold(const xpbd6_state* s, float margin, void* stream);
+/* kernels_6dof.py:159-211 + 386-430 + 441-483: floor, box manifold and joint
+ * projections accumulated into acc_x / acc_r in one pass. */
+int xpbd6_solve_positions(const xpbd6_state* s, const xpbd6_params* p, int first, void* stream);
+/* kernels_6dof.py:487-506 apply_jacobi_6dof */
+int xpbd6_apply_jacobi(const xpbd6_state* s, float relax, void* stream);
+/* kernels_6dof.py:513-535 finalize_velocity_6dof */
+int xpbd6_finalize(const xpbd6_state* s, const xpbd6_params* p, void* stream);
+/* kernels_6dof.py:542-659 velocity_floor + velocity_box */
+int xpbd6_solve_velocities(const xpbd6_state* s, const xpbd6_params* p, void* stream);
+/* kernels_6dof.py:663-691 apply_velocity_6dof + cap_velocity_6dof */
+int xpbd6_apply_velocity(const xpbd6_state* s, const xpbd6_params* p, void* stream);
+/* kernels_bvh.py:22-48 compute_body_aabb (lowers/uppers float4[n]) */
+int xpbd6_body_aabb(const xpbd6_state* s, const xpbd6_params* p, float* lowers, float* uppers,
+                    void* stream);
+
+typedef struct xpbd6_solver xpbd6_solver;
+int xpbd6_create(xpbd6_solver** out);
+int xpbd6_destroy(xpbd6_solver* h);
+int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_params* p);
+/* solver_6dof.py:428-479 + 232-258 broad phase: writes the pair list sorted by
+ * (a, b) (lbvh, hashgrid) or in grid order (grid) and the live count. */
+int xpbd6_broadphase(xpbd6_solver* h, void* stream);
+/* solver_6dof.py:357-426 _record: the substep loop on the current pair list. */
+int xpbd6_substeps(xpbd6_solver* h, void* stream);
+/* broad phase + substeps, captured as one CUDA graph per frame. */
+int xpbd6_step(xpbd6_solver* h, int frames, void* stream);
+int xpbd6_status(xpbd6_solver* h, int* out, void* stream);
+/* Morton keys of the LBVH over lowers/uppers (float4[n]) -> uint32[n]. */
+int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XPBD_B200_H */

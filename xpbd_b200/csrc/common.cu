@@ -1,0 +1,102 @@
+// Library-wide host utilities: version, error capture, device queries and the
+// host-side constraint coloring (coloring.py:26-89).
+#include <algorithm>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace xpbd {
+
+static std::mutex g_err_mu;
+static std::string g_last_error;
+
+void set_last_error(const char* where, cudaError_t e) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+}
+
+int num_sms() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 1;
+  }
+  return sms;
+}
+
+}  // namespace xpbd
+
+extern "C" const char* xpbd_version(void) { return "xpbd_b200 0.1 (sm_100a)"; }
+
+extern "C" const char* xpbd_last_error(void) {
+  std::lock_guard<std::mutex> lk(xpbd::g_err_mu);
+  return xpbd::g_last_error.c_str();
+}
+
+// coloring.py:26-71 color_constraints.  Rows are visited in a stable order of
+// decreasing (deg a + deg b) (Welsh-Powell); each takes the smallest color not
+// used by a row already touching either endpoint.  Per-body used colors are kept
+// as a growing bitset, so a row costs O(colors / 64).
+extern "C" int xpbd_color_constraints(int n_bodies, int m, const int* a, const int* b, int* color) {
+  if (m < 0 || n_bodies < 0 || (m > 0 && (!a || !b || !color))) return -1;
+  if (m == 0) return 0;
+  std::vector<long long> deg((size_t)std::max(n_bodies, 1), 0);
+  for (int j = 0; j < m; ++j) {
+    if (a[j] < 0 || a[j] >= n_bodies || b[j] >= n_bodies) return -1;
+    deg[a[j]] += 1;
+    if (b[j] >= 0) deg[b[j]] += 1;
+  }
+  std::vector<long long> key(m);
+  for (int j = 0; j < m; ++j) key[j] = -(deg[a[j]] + (b[j] >= 0 ? deg[b[j]] : 0));
+  std::vector<int> order(m);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int p, int q) { return key[p] < key[q]; });
+  std::vector<std::vector<uint64_t>> used((size_t)std::max(n_bodies, 1));
+  int k = 0;
+  for (int t = 0; t < m; ++t) {
+    int j = order[t];
+    const std::vector<uint64_t>& ua = used[a[j]];
+    static const std::vector<uint64_t> empty;
+    const std::vector<uint64_t>& ub = b[j] >= 0 ? used[b[j]] : empty;
+    size_t words = std::max(ua.size(), ub.size());
+    int c = -1;
+    for (size_t w = 0; w < words && c < 0; ++w) {
+      uint64_t occ = (w < ua.size() ? ua[w] : 0ull) | (w < ub.size() ? ub[w] : 0ull);
+      if (occ != ~0ull) c = (int)(w * 64 + __builtin_ctzll(~occ));
+    }
+    if (c < 0) c = (int)(words * 64);
+    color[j] = c;
+    k = std::max(k, c + 1);
+    size_t word = (size_t)c / 64;
+    uint64_t bit = 1ull << (c % 64);
+    for (int e = 0; e < 2; ++e) {
+      int body = e == 0 ? a[j] : b[j];
+      if (body < 0) continue;
+      std::vector<uint64_t>& u = used[body];
+      if (u.size() <= word) u.resize(word + 1, 0ull);
+      u[word] |= bit;
+    }
+  }
+  return k;
+}
+
+// coloring.py:74-89 color_ranges: stable sort of row ids by color + CSR starts.
+extern "C" int xpbd_color_ranges(int m, const int* color, int* order, int* starts) {
+  if (m < 0 || (m > 0 && (!color || !order || !starts))) return -1;
+  int k = 0;
+  for (int j = 0; j < m; ++j) {
+    if (color[j] < 0) return -1;
+    k = std::max(k, color[j] + 1);
+  }
+  std::vector<int> cnt((size_t)k + 1, 0);
+  for (int j = 0; j < m; ++j) cnt[color[j] + 1] += 1;
+  for (int c = 0; c < k; ++c) cnt[c + 1] += cnt[c];
+  for (int c = 0; c <= k; ++c) starts[c] = cnt[c];
+  for (int j = 0; j < m; ++j) order[cnt[color[j]]++] = j;
+  return k;
+}

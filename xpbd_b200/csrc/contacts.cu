@@ -1,0 +1,342 @@
+// Sphere-sphere contact generation for the 3-DOF solver, on the device.
+//
+// Replaces the reference's per-frame host round trip (solver.py:412-416:
+// _sanitize_positions solver.py:469-483, _rebuild_contacts solver.py:275-342,
+// _grid_candidate_pairs solver.py:514-562) and produces the same CONTACT rows
+// in the same order:
+//   1. non-finite positions are reset to their initial values (velocity 0);
+//   2. margin = min(contact_margin + 3 dt max|v_component|, r_max) (fp64),
+//      cell = 2 r_max + margin, each collidable sphere k gets integer cell
+//      coordinates floor(p / cell) (fp32) shifted by the per-axis minimum, and
+//      the linear id cid = (cx S + cy) S + cz with S = max extent + 2;
+//   3. spheres are sorted by cid (stable, so ties keep ascending index);
+//   4. for each of the 14 forward cell offsets o and each sphere k, the spheres
+//      of cell cid_k + delta_o are visited in sorted order, and a pair is kept
+//      if it overlaps within the margin and is not already joined by a row;
+//   5. counts per (o, k) are scanned, and the pairs are written at their scan
+//      offsets -- offset-major, then k, then partner: the reference's order.
+#include <algorithm>
+
+#include "prims.cuh"
+
+namespace xpbd {
+
+__constant__ int kFwd[14][3] = {{0, 0, 0},  {1, -1, -1}, {1, -1, 0}, {1, -1, 1}, {1, 0, -1},
+                                {1, 0, 0},  {1, 0, 1},   {1, 1, -1}, {1, 1, 0},  {1, 1, 1},
+                                {0, 1, -1}, {0, 1, 0},   {0, 1, 1},  {0, 0, 1}};
+
+struct ContactRed {
+  int cmin[3];
+  int cmax[3];
+  int vmax_bits;  // max |v component| as float bits (non-negative)
+  int pad;
+};
+
+struct ContactArgs {
+  float4* x;
+  float4* v;
+  const float4* x_init;
+  const float* radius;
+  const float* friction;
+  const int* coll;
+  const int64_t* existing;
+  int n_existing;
+  int n, m;            // bodies, collidable spheres
+  double contact_margin, dt, rmax;
+  int4* ri;
+  float4* rf;
+  float4* ra;
+  int* n_rows;
+  int n_static, cap_contacts;
+  int* status;
+};
+
+struct ContactScratch {
+  ContactRed* red;
+  int4* cell;          // per collidable: cell coords (unshifted)
+  int64_t* cid;        // per collidable
+  uint64_t* skey;      // sorted cid
+  uint32_t* sval;      // sorted local index
+  int* counts;         // 14 m
+  int* offsets;        // 14 m
+  int* total;
+  void* sort_tmp;
+  void* scan_tmp;
+};
+
+__global__ void kc_init(ContactRed* r) {
+  if (threadIdx.x == 0) {
+    for (int d = 0; d < 3; ++d) {
+      r->cmin[d] = 0x7fffffff;
+      r->cmax[d] = (int)0x80000000;
+    }
+    r->vmax_bits = 0;
+  }
+}
+
+XD bool finite3(float4 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+
+// solver.py:469-483 + the max |v| of solver.py:309
+__global__ void kc_sanitize(ContactArgs a, ContactRed* red) {
+  float vm = 0.0f;
+  for (int i = gtid(); i < a.n; i += gstride()) {
+    float4 xi = a.x[i];
+    if (!finite3(xi)) {
+      float4 x0 = a.x_init[i];
+      a.x[i] = make_float4(x0.x, x0.y, x0.z, xi.w);
+      a.v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      raise_status(a.status, XPBD_ERR_NAN);
+    }
+    float4 vi = a.v[i];
+    vm = fmaxf(vm, fmaxf(fabsf(vi.x), fmaxf(fabsf(vi.y), fabsf(vi.z))));
+  }
+  for (int o = 16; o; o >>= 1) vm = fmaxf(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&red->vmax_bits, __float_as_int(vm));
+}
+
+XD void margin_cell(const ContactArgs& a, const ContactRed* red, float* cell_f, float* margin_f) {
+  double vmax = (double)__int_as_float(red->vmax_bits);
+  double margin = a.contact_margin + 3.0 * a.dt * vmax;
+  if (a.rmax < margin) margin = a.rmax;  // python min(margin, rmax)
+  *cell_f = (float)(a.rmax * 2.0 + margin);
+  *margin_f = (float)margin;
+}
+
+__global__ void kc_cells(ContactArgs a, ContactScratch s) {
+  float cell, marg;
+  margin_cell(a, s.red, &cell, &marg);
+  int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (int k = gtid(); k < a.m; k += gstride()) {
+    float4 p = a.x[a.coll[k]];
+    int c[3] = {(int)floorf(p.x / cell), (int)floorf(p.y / cell), (int)floorf(p.z / cell)};
+    s.cell[k] = make_int4(c[0], c[1], c[2], 0);
+    for (int d = 0; d < 3; ++d) {
+      lmin[d] = min(lmin[d], c[d]);
+      lmax[d] = max(lmax[d], c[d]);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o; o >>= 1) {
+      lmin[d] = min(lmin[d], __shfl_xor_sync(0xffffffffu, lmin[d], o));
+      lmax[d] = max(lmax[d], __shfl_xor_sync(0xffffffffu, lmax[d], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&s.red->cmin[d], lmin[d]);
+      atomicMax(&s.red->cmax[d], lmax[d]);
+    }
+  }
+}
+
+XD int64_t grid_S(const ContactRed* r) {
+  int64_t ext = 0;
+  for (int d = 0; d < 3; ++d) ext = max(ext, (int64_t)r->cmax[d] - (int64_t)r->cmin[d]);
+  return ext + 2;
+}
+
+__global__ void kc_keys(ContactArgs a, ContactScratch s) {
+  int64_t S = grid_S(s.red);
+  for (int k = gtid(); k < a.m; k += gstride()) {
+    int4 c = s.cell[k];
+    int64_t cx = (int64_t)c.x - s.red->cmin[0], cy = (int64_t)c.y - s.red->cmin[1],
+            cz = (int64_t)c.z - s.red->cmin[2];
+    int64_t id = (cx * S + cy) * S + cz;
+    s.cid[k] = id;
+    s.skey[k] = (uint64_t)id;
+    s.sval[k] = (uint32_t)k;
+  }
+}
+
+XD int lower_bound_u64(const uint64_t* s, int m, uint64_t t) {
+  int lo = 0, hi = m;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (s[mid] < t) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+XD bool has_key(const int64_t* keys, int nk, int64_t key) {
+  int lo = 0, hi = nk;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (keys[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return lo < nk && keys[lo] == key;
+}
+
+// Visits the kept pairs of slot (o, k) in order; `emit(rank, a, b)` per pair.
+template <class Emit>
+XD int visit_slot(const ContactArgs& a, const ContactScratch& s, int o, int k, float margin_f,
+                  int64_t S, Emit emit) {
+  int64_t delta = ((int64_t)kFwd[o][0] * S + kFwd[o][1]) * S + kFwd[o][2];
+  int64_t target = s.cid[k] + delta;
+  if (target < 0) return 0;
+  int q = lower_bound_u64(s.skey, a.m, (uint64_t)target);
+  int cnt = 0;
+  const int ga = a.coll[k];
+  const float4 pa = a.x[ga];
+  const float ra = a.radius[ga];
+  for (; q < a.m && s.skey[q] == (uint64_t)target; ++q) {
+    int partner = (int)s.sval[q];
+    if (o == 0 && !(partner > k)) continue;
+    int gb = a.coll[partner];
+    float4 pb = a.x[gb];
+    float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
+    float d2 = dx * dx + dy * dy + dz * dz;
+    float rs = ra + a.radius[gb] + margin_f;
+    if (!(d2 <= rs * rs)) continue;
+    if (a.n_existing) {
+      int64_t key = ga < gb ? (int64_t)ga * a.n + gb : (int64_t)gb * a.n + ga;
+      if (has_key(a.existing, a.n_existing, key)) continue;
+    }
+    emit(cnt, ga, gb);
+    ++cnt;
+  }
+  return cnt;
+}
+
+__global__ void kc_count(ContactArgs a, ContactScratch s) {
+  float cell, marg;
+  margin_cell(a, s.red, &cell, &marg);
+  int64_t S = grid_S(s.red);
+  for (int t = gtid(); t < 14 * a.m; t += gstride()) {
+    int o = t / a.m, k = t - o * a.m;
+    s.counts[t] = visit_slot(a, s, o, k, marg, S, [](int, int, int) {});
+  }
+}
+
+__global__ void kc_write(ContactArgs a, ContactScratch s) {
+  float cell, marg;
+  margin_cell(a, s.red, &cell, &marg);
+  int64_t S = grid_S(s.red);
+  const int total = *s.total;
+  if (gtid() == 0) {
+    int live = min(total, a.cap_contacts);
+    *a.n_rows = a.n_static + live;
+    if (total > a.cap_contacts) raise_status(a.status, XPBD_ERR_OVERFLOW);
+  }
+  for (int t = gtid(); t < 14 * a.m; t += gstride()) {
+    if (s.counts[t] == 0) continue;
+    int o = t / a.m, k = t - o * a.m;
+    int base = s.offsets[t];
+    visit_slot(a, s, o, k, marg, S, [&](int r, int ga, int gb) {
+      int slot = base + r;
+      if (slot >= a.cap_contacts) return;
+      int row = a.n_static + slot;
+      a.ri[row] = make_int4(XPBD_CONTACT, ga, gb, 1);
+      a.rf[row] = make_float4(a.radius[ga] + a.radius[gb], 0.0f, sqrtf(a.friction[ga] * a.friction[gb]), 0.0f);
+      a.ra[row] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    });
+  }
+}
+
+__global__ void kc_no_contacts(ContactArgs a) {
+  if (gtid() == 0) *a.n_rows = a.n_static;
+}
+
+}  // namespace xpbd
+
+using namespace xpbd;
+
+struct xpbd3_contacts {
+  int n = 0, m = 0;
+  void* buf = nullptr;
+  ContactScratch s{};
+};
+
+extern "C" int xpbd3_contacts_create(xpbd3_contacts** out, int n_bodies, int n_collide) {
+  if (!out || n_bodies < 0 || n_collide < 0 || n_collide > n_bodies) return XPBD_ERR_BAD_ARG;
+  xpbd3_contacts* c = new xpbd3_contacts();
+  c->n = n_bodies;
+  c->m = n_collide;
+  int m = std::max(n_collide, 1);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  size_t o_red = take(sizeof(ContactRed)), o_cell = take(sizeof(int4) * m), o_cid = take(8 * (size_t)m),
+         o_skey = take(8 * (size_t)m), o_sval = take(4 * (size_t)m), o_cnt = take(4 * 14 * (size_t)m),
+         o_off = take(4 * 14 * (size_t)m), o_tot = take(16), o_st = take(sort_scratch_bytes(m)),
+         o_sc = take(scan_scratch_bytes(14 * m));
+  cudaError_t e = cudaMalloc(&c->buf, off);
+  if (e != cudaSuccess) {
+    set_last_error("cudaMalloc", e);
+    delete c;
+    return XPBD_ERR_CUDA;
+  }
+  char* b = static_cast<char*>(c->buf);
+  c->s.red = reinterpret_cast<ContactRed*>(b + o_red);
+  c->s.cell = reinterpret_cast<int4*>(b + o_cell);
+  c->s.cid = reinterpret_cast<int64_t*>(b + o_cid);
+  c->s.skey = reinterpret_cast<uint64_t*>(b + o_skey);
+  c->s.sval = reinterpret_cast<uint32_t*>(b + o_sval);
+  c->s.counts = reinterpret_cast<int*>(b + o_cnt);
+  c->s.offsets = reinterpret_cast<int*>(b + o_off);
+  c->s.total = reinterpret_cast<int*>(b + o_tot);
+  c->s.sort_tmp = b + o_st;
+  c->s.scan_tmp = b + o_sc;
+  *out = c;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_contacts_destroy(xpbd3_contacts* c) {
+  if (!c) return XPBD_OK;
+  if (c->buf) cudaFree(c->buf);
+  delete c;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_contacts_build(xpbd3_contacts* c, const xpbd3_state* st, const float* radius,
+                                    const float* friction, const int* collide_idx, int n_collide,
+                                    const int64_t* existing, int n_existing, const float* x_init,
+                                    double contact_margin, double dt, double r_max, int* status_dev,
+                                    void* stream) {
+  if (!c || !st || n_collide != c->m || st->n_bodies != c->n || !x_init || !radius || !friction ||
+      (n_collide > 0 && !collide_idx) || (n_existing > 0 && !existing) || !st->n_rows)
+    return XPBD_ERR_BAD_ARG;
+  cudaStream_t s = as_stream(stream);
+  ContactArgs a{};
+  a.x = reinterpret_cast<float4*>(st->x);
+  a.v = reinterpret_cast<float4*>(st->v);
+  a.x_init = reinterpret_cast<const float4*>(x_init);
+  a.radius = radius;
+  a.friction = friction;
+  a.coll = collide_idx;
+  a.existing = existing;
+  a.n_existing = n_existing;
+  a.n = st->n_bodies;
+  a.m = n_collide;
+  a.contact_margin = contact_margin;
+  a.dt = dt;
+  a.rmax = r_max;
+  a.ri = reinterpret_cast<int4*>(st->row_i);
+  a.rf = reinterpret_cast<float4*>(st->row_f);
+  a.ra = reinterpret_cast<float4*>(st->row_anchor);
+  a.n_rows = st->n_rows;
+  a.n_static = st->n_rows_static;
+  a.cap_contacts = st->row_capacity - st->n_rows_static;
+  a.status = status_dev;
+  if (a.n == 0) return XPBD_OK;
+  kc_init<<<1, 32, 0, s>>>(c->s.red);
+  kc_sanitize<<<stream_blocks(a.n, 256), 256, 0, s>>>(a, c->s.red);
+  if (a.m < 2) {
+    kc_no_contacts<<<1, 32, 0, s>>>(a);
+    XPBD_LAUNCHED();
+    return XPBD_OK;
+  }
+  int blocks_m = stream_blocks(a.m, 256);
+  kc_cells<<<blocks_m, 256, 0, s>>>(a, c->s);
+  kc_keys<<<blocks_m, 256, 0, s>>>(a, c->s);
+  XPBD_LAUNCHED();
+  int rc = sort_pairs_u64(c->s.skey, c->s.sval, a.m, c->s.sort_tmp, 63, s);
+  if (rc) return rc;
+  int blocks_t = stream_blocks(14LL * a.m, 128);
+  kc_count<<<blocks_t, 128, 0, s>>>(a, c->s);
+  rc = exclusive_scan_i32(c->s.counts, c->s.offsets, 14 * a.m, c->s.total, c->s.scan_tmp, s);
+  if (rc) return rc;
+  kc_write<<<blocks_t, 128, 0, s>>>(a, c->s);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}

@@ -1,0 +1,104 @@
+// Shared engine utilities: status word, bounded grid barrier for persistent
+// cooperative kernels, launch helpers and error capture.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/xpbd_b200.h"
+#include "xpbd_math.cuh"
+
+namespace xpbd {
+
+// ---- error capture ------------------------------------------------------------
+void set_last_error(const char* where, cudaError_t e);
+#define XPBD_CUDA(call)                                  \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) {                             \
+      ::xpbd::set_last_error(#call, e_);                 \
+      return XPBD_ERR_CUDA;                              \
+    }                                                    \
+  } while (0)
+#define XPBD_LAUNCHED()                                  \
+  do {                                                   \
+    cudaError_t e_ = cudaGetLastError();                 \
+    if (e_ != cudaSuccess) {                             \
+      ::xpbd::set_last_error("kernel launch", e_);       \
+      return XPBD_ERR_CUDA;                              \
+    }                                                    \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int num_sms();
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+// Grid size for a streaming kernel over `n` items: at most 4 waves of `threads`.
+inline int stream_blocks(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  long long cap = (long long)num_sms() * 8;
+  if (b > cap) b = cap;
+  return (int)(b < 1 ? 1 : b);
+}
+
+// ---- device status word ---------------------------------------------------------
+XD void raise_status(int* status, int bits) {
+  if (status) atomicOr(status, bits);
+}
+
+XD uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// ---- bounded grid barrier --------------------------------------------------------
+// Generation-counting barrier for a cooperative launch (all blocks co-resident).
+// Every wait gives up after ~2 s of wall time, sets XPBD_ERR_BARRIER_TIMEOUT in
+// the status word and returns; once the bit is set no barrier waits again, so a
+// kernel can never hang on it.  With one block it is a plain __syncthreads().
+struct GridBarrier {
+  unsigned* count;  // arrivals at the current barrier
+  unsigned* gen;    // generation number
+  int* status;
+};
+
+constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;
+
+XD void grid_sync(const GridBarrier& b) {
+  if (gridDim.x == 1) {
+    __syncthreads();
+    return;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = b.gen;
+    volatile int* vstat = b.status;
+    unsigned g = *vgen;
+    __threadfence();
+    unsigned prev = atomicAdd(b.count, 1u);
+    if (prev == gridDim.x - 1) {
+      atomicExch(b.count, 0u);
+      __threadfence();
+      atomicAdd(b.gen, 1u);
+    } else if ((*vstat & XPBD_ERR_BARRIER_TIMEOUT) == 0) {
+      uint64_t t0 = global_ns();
+      while (*vgen == g) {
+        if (*vstat & XPBD_ERR_BARRIER_TIMEOUT) break;
+        if (global_ns() - t0 > kBarrierTimeoutNs) {
+          atomicOr(b.status, XPBD_ERR_BARRIER_TIMEOUT);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// grid-stride helpers
+XD int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+XD int gstride() { return gridDim.x * blockDim.x; }
+
+}  // namespace xpbd

@@ -1,0 +1,630 @@
+// 3-DOF particle XPBD engine (replaces src/xpbd3d/kernels.py and the device
+// part of Solver.step, solver.py:412-467).
+//
+// Layout: particles are float4 records (position + inverse mass, velocity,
+// substep-start position, Jacobi accumulator dx + count); rows are int4
+// (type, a, b, active) + float4 (rest, compliance, mu, floor y) + float4
+// (ATTACH anchor) + float lambda.
+//
+// Drivers
+//  * per-kernel entry points (one launch per reference kernel) for parity tests;
+//  * `k3_frames`: one persistent launch runs whole frames.  Phases (integrate,
+//    row projection, averaged apply, finalize + clamp) are separated by a block
+//    barrier when one CTA holds the scene, else by a bounded grid barrier of a
+//    cooperative launch.  When the particle state fits in shared memory the
+//    single-CTA variant stages it there for the whole launch and accumulates
+//    Jacobi corrections with shared-memory atomics instead of global atomics.
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace xpbd {
+
+struct Dev3 {
+  float4* x;
+  float4* v;
+  float4* xp;
+  float4* acc;
+  float* lam;
+  const int4* ri;
+  const float4* rf;
+  const float4* ra;
+  const int* n_rows;
+  const int* corder;
+  const int* cstarts;
+  int n;
+  int ncolors;
+};
+
+struct Par3 {
+  float h, gx, gy, gz, damping, relax, max_speed;
+  int cap_on, substeps, iterations, gs;
+};
+
+// ---------------------------------------------------------------------------
+// kernels.py:80-98 friction_delta
+XD V3 friction_delta(V3 dp_rel, V3 n_hat, float penetration, float mu) {
+  V3 dp_t = dp_rel - n_hat * dot(dp_rel, n_hat);
+  float lt = length(dp_t);
+  if (lt < kEps) return V3{0.0f, 0.0f, 0.0f};
+  float scale = 1.0f;
+  float cone = mu * penetration;
+  if (lt >= cone) scale = cone / lt;
+  return dp_t * (-scale);
+}
+
+// kernels.py:49-73 integrate
+XD void body_integrate(float4* x, float4* v, float4* xp, int i, float h, V3 g) {
+  float4 xi = x[i];
+  xp[i] = make_float4(xi.x, xi.y, xi.z, 0.0f);
+  if (xi.w == 0.0f) return;
+  V3 vi = v3(v[i]) + g * h;
+  v[i] = f4(vi, 0.0f);
+  x[i] = f4(v3(xi) + vi * h, xi.w);
+}
+
+// kernels.py:326-339 apply_jacobi
+XD void body_apply(float4* x, float4* acc, int i, float relax) {
+  float4 a = acc[i];
+  int c = (int)a.w;
+  if (c > 0) {
+    float4 xi = x[i];
+    if (xi.w > 0.0f) x[i] = f4(v3(xi) + v3(a) * (relax / (float)c), xi.w);
+  }
+  acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// kernels.py:346-371 finalize_velocity + cap_velocity
+XD void body_finalize(const float4* x, const float4* xp, float4* v, int i, float h, float damping,
+                      int cap_on, float max_speed) {
+  float4 xi = x[i];
+  V3 vi;
+  if (xi.w == 0.0f) {
+    vi = V3{0.0f, 0.0f, 0.0f};
+  } else {
+    vi = ((v3(xi) - v3(xp[i])) / h) * (1.0f - damping);
+  }
+  if (cap_on) {
+    float sp = length(vi);
+    if (sp > max_speed) vi = vi * (max_speed / sp);
+  }
+  v[i] = f4(vi, 0.0f);
+}
+
+// kernels.py:219-322 solve_constraints_jacobi, one row.  `acc(i, d)` adds the
+// correction d (and one to the count) to particle i.
+template <bool FIRST, class Acc>
+XD void row_jacobi(const float4* x, const float4* xp, const int4* ri, const float4* rf,
+                   const float4* ra, float* lam, int j, float h, Acc acc) {
+  int4 r = ri[j];
+  float lam_old = FIRST ? 0.0f : lam[j];
+  float lam_new = lam_old;
+  if (r.w != 0) {
+    int t = r.x;
+    if (t == XPBD_DISTANCE || t == XPBD_ATTACH) {
+      float inv_dt2 = 1.0f / (h * h);
+      int a = r.y;
+      float4 xa = x[a];
+      float wa = xa.w, wb;
+      V3 pb;
+      if (t == XPBD_ATTACH) {
+        pb = v3(ra[j]);
+        wb = 0.0f;
+      } else {
+        float4 xb = x[r.z];
+        pb = v3(xb);
+        wb = xb.w;
+      }
+      float wsum = wa + wb;
+      if (wsum != 0.0f) {
+        V3 d = v3(xa) - pb;
+        float L = length(d);
+        if (!(L < kEps)) {
+          V3 n_hat = d / L;
+          float4 f = rf[j];
+          float C = L - f.x;
+          float alpha = f.y * inv_dt2;
+          float dlam = (-C - alpha * lam_old) / (wsum + alpha);
+          lam_new = lam_old + dlam;
+          acc(a, n_hat * (wa * dlam));
+          if (t == XPBD_DISTANCE) acc(r.z, (-n_hat) * (wb * dlam));
+        }
+      }
+    } else if (t == XPBD_FLOOR) {
+      int a = r.y;
+      float4 xa = x[a];
+      float wa = xa.w;
+      if (wa != 0.0f) {
+        float4 f = rf[j];
+        float C = xa.y - f.w;
+        if (!(C >= 0.0f)) {
+          float dlam = -C / wa;
+          lam_new = lam_old + dlam;
+          V3 corr = V3{0.0f, wa * dlam, 0.0f};
+          float mu = f.z;
+          if (mu > 0.0f) {
+            V3 dp_rel = (v3(xa) + corr) - v3(xp[a]);
+            corr = corr + friction_delta(dp_rel, V3{0.0f, 1.0f, 0.0f}, -C, mu);
+          }
+          acc(a, corr);
+        }
+      }
+    } else if (t == XPBD_CONTACT) {
+      int a = r.y, b = r.z;
+      float4 xa = x[a], xb = x[b];
+      float wa = xa.w, wb = xb.w;
+      float wsum = wa + wb;
+      if (wsum != 0.0f) {
+        V3 d = v3(xa) - v3(xb);
+        float L = length(d);
+        if (!(L < kEps)) {
+          V3 n_hat = d / L;
+          float4 f = rf[j];
+          float C = L - f.x;
+          if (!(C >= 0.0f)) {
+            float dlam = -C / wsum;
+            lam_new = lam_old + dlam;
+            V3 ca = n_hat * (wa * dlam);
+            V3 cb = (-n_hat) * (wb * dlam);
+            float mu = f.z;
+            if (mu > 0.0f) {
+              V3 dp_rel = ((v3(xa) + ca) - v3(xp[a])) - ((v3(xb) + cb) - v3(xp[b]));
+              V3 fc = friction_delta(dp_rel, n_hat, -C, mu);
+              ca = ca + fc * (wa / wsum);
+              cb = cb - fc * (wb / wsum);
+            }
+            acc(a, ca);
+            acc(b, cb);
+          }
+        }
+      }
+    }
+  }
+  if (FIRST || lam_new != lam_old) lam[j] = lam_new;
+}
+
+XD void put3(float4* x, int i, V3 p) { x[i] = f4(p, x[i].w); }
+
+// kernels.py:105-208 solve_constraints_color, one row, in place.
+template <bool FIRST>
+XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, const float4* ra,
+               float* lam, int j, float h) {
+  int4 r = ri[j];
+  float lam_old = FIRST ? 0.0f : lam[j];
+  float lam_new = lam_old;
+  if (r.w != 0) {
+    int t = r.x;
+    if (t == XPBD_DISTANCE || t == XPBD_ATTACH) {
+      float inv_dt2 = 1.0f / (h * h);
+      int a = r.y;
+      float4 xa = x[a];
+      float wa = xa.w, wb;
+      V3 pb;
+      if (t == XPBD_ATTACH) {
+        pb = v3(ra[j]);
+        wb = 0.0f;
+      } else {
+        float4 xb = x[r.z];
+        pb = v3(xb);
+        wb = xb.w;
+      }
+      float wsum = wa + wb;
+      if (wsum != 0.0f) {
+        V3 d = v3(xa) - pb;
+        float L = length(d);
+        if (!(L < kEps)) {
+          V3 n_hat = d / L;
+          float4 f = rf[j];
+          float C = L - f.x;
+          float alpha = f.y * inv_dt2;
+          float dlam = (-C - alpha * lam_old) / (wsum + alpha);
+          lam_new = lam_old + dlam;
+          put3(x, a, v3(xa) + n_hat * (wa * dlam));
+          if (t == XPBD_DISTANCE) put3(x, r.z, v3(x[r.z]) - n_hat * (wb * dlam));
+        }
+      }
+    } else if (t == XPBD_FLOOR) {
+      int a = r.y;
+      float4 xa = x[a];
+      float wa = xa.w;
+      if (wa != 0.0f) {
+        float4 f = rf[j];
+        float C = xa.y - f.w;
+        if (!(C >= 0.0f)) {
+          float dlam = -C / wa;
+          lam_new = lam_old + dlam;
+          V3 pa = v3(xa) + V3{0.0f, wa * dlam, 0.0f};
+          float mu = f.z;
+          if (mu > 0.0f) {
+            V3 dp_rel = pa - v3(xp[a]);
+            pa = pa + friction_delta(dp_rel, V3{0.0f, 1.0f, 0.0f}, -C, mu);
+          }
+          put3(x, a, pa);
+        }
+      }
+    } else if (t == XPBD_CONTACT) {
+      int a = r.y, b = r.z;
+      float4 xa = x[a], xb = x[b];
+      float wa = xa.w, wb = xb.w;
+      float wsum = wa + wb;
+      if (wsum != 0.0f) {
+        V3 d = v3(xa) - v3(xb);
+        float L = length(d);
+        if (!(L < kEps)) {
+          V3 n_hat = d / L;
+          float4 f = rf[j];
+          float C = L - f.x;
+          if (!(C >= 0.0f)) {
+            float dlam = -C / wsum;
+            lam_new = lam_old + dlam;
+            V3 pa = v3(xa) + n_hat * (wa * dlam);
+            V3 pb = v3(xb) - n_hat * (wb * dlam);
+            float mu = f.z;
+            if (mu > 0.0f) {
+              V3 dp_rel = (pa - v3(xp[a])) - (pb - v3(xp[b]));
+              V3 corr = friction_delta(dp_rel, n_hat, -C, mu);
+              pa = pa + corr * (wa / wsum);
+              pb = pb - corr * (wb / wsum);
+            }
+            put3(x, a, pa);
+            put3(x, b, pb);
+          }
+        }
+      }
+    }
+  }
+  if (FIRST || lam_new != lam_old) lam[j] = lam_new;
+}
+
+struct AccGlobal {
+  float4* acc;
+  XD void operator()(int i, V3 d) const { red_add4(acc + i, make_float4(d.x, d.y, d.z, 1.0f)); }
+};
+struct AccShared {
+  float4* acc;  // shared-memory array
+  XD void operator()(int i, V3 d) const { red_add3w(acc + i, d, 1.0f); }
+};
+
+// ---------------------------------------------------------------------------
+// per-kernel entry points
+__global__ void k3_integrate(Dev3 s, float h, float gx, float gy, float gz) {
+  for (int i = gtid(); i < s.n; i += gstride()) body_integrate(s.x, s.v, s.xp, i, h, V3{gx, gy, gz});
+}
+template <bool FIRST>
+__global__ void k3_jacobi(Dev3 s, float h) {
+  int m = *s.n_rows;
+  AccGlobal acc{s.acc};
+  for (int j = gtid(); j < m; j += gstride())
+    row_jacobi<FIRST>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, j, h, acc);
+}
+__global__ void k3_apply(Dev3 s, float relax) {
+  for (int i = gtid(); i < s.n; i += gstride()) body_apply(s.x, s.acc, i, relax);
+}
+template <bool FIRST>
+__global__ void k3_color(Dev3 s, int start, int count, float h) {
+  for (int t = gtid(); t < count; t += gstride())
+    row_gs<FIRST>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, s.corder[start + t], h);
+}
+__global__ void k3_finalize(Dev3 s, float h, float damping) {
+  for (int i = gtid(); i < s.n; i += gstride()) body_finalize(s.x, s.xp, s.v, i, h, damping, 0, 0.0f);
+}
+__global__ void k3_cap(Dev3 s, float max_speed) {
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    V3 vi = v3(s.v[i]);
+    float sp = length(vi);
+    if (sp > max_speed) s.v[i] = f4(vi * (max_speed / sp), 0.0f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent frame kernel.  SMEM: one CTA stages particles (x, v, x_prev, acc)
+// and multipliers in shared memory.  Otherwise the state stays in global
+// memory (L2-resident for these sizes) and phases are separated by the
+// bounded grid barrier of a cooperative launch.
+template <bool GS, bool SMEM>
+__global__ void __launch_bounds__(1024) k3_frames(Dev3 g, Par3 p, int frames, GridBarrier bar) {
+  extern __shared__ float4 smem[];
+  const int n = g.n;
+  const int m = *g.n_rows;
+  Dev3 s = g;
+  if (SMEM) {
+    s.x = smem;
+    s.v = smem + n;
+    s.xp = smem + 2 * n;
+    s.acc = smem + 3 * n;
+    s.lam = reinterpret_cast<float*>(smem + 4 * n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      s.x[i] = g.x[i];
+      s.v[i] = g.v[i];
+      s.xp[i] = g.xp[i];
+      s.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    for (int j = threadIdx.x; j < m; j += blockDim.x) s.lam[j] = g.lam[j];
+    __syncthreads();
+  }
+  const V3 gv = V3{p.gx, p.gy, p.gz};
+  const int tid0 = SMEM ? threadIdx.x : gtid();
+  const int stride = SMEM ? blockDim.x : gstride();
+  auto sync = [&]() {
+    if (SMEM) __syncthreads(); else grid_sync(bar);
+  };
+  auto acc_fn = [&](int i, V3 d) {
+    if (SMEM) AccShared{s.acc}(i, d); else AccGlobal{s.acc}(i, d);
+  };
+  if (m > 0 && p.iterations == 0) {
+    for (int j = tid0; j < m; j += stride) s.lam[j] = 0.0f;
+  }
+  for (int f = 0; f < frames; ++f) {
+    for (int i = tid0; i < n; i += stride) body_integrate(s.x, s.v, s.xp, i, p.h, gv);
+    sync();
+    for (int sub = 0; sub < p.substeps; ++sub) {
+      const bool more = (sub + 1 < p.substeps);  // integrate the next substep in this frame
+      if (m > 0) {
+        for (int it = 0; it < p.iterations; ++it) {
+          if (GS) {
+            for (int c = 0; c < g.ncolors; ++c) {
+              int start = g.cstarts[c], count = g.cstarts[c + 1] - start;
+              for (int t = tid0; t < count; t += stride) {
+                int j = g.corder[start + t];
+                if (it == 0) row_gs<true>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h);
+                else row_gs<false>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h);
+              }
+              sync();
+            }
+          } else {
+            for (int j = tid0; j < m; j += stride) {
+              if (it == 0) row_jacobi<true>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
+              else row_jacobi<false>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
+            }
+            sync();
+            if (it + 1 < p.iterations) {
+              for (int i = tid0; i < n; i += stride) body_apply(s.x, s.acc, i, p.relax);
+              sync();
+            }
+          }
+        }
+      }
+      // last apply (Jacobi) + finalize + clamp + the next substep's integrate, per body
+      for (int i = tid0; i < n; i += stride) {
+        if (!GS && m > 0 && p.iterations > 0) body_apply(s.x, s.acc, i, p.relax);
+        body_finalize(s.x, s.xp, s.v, i, p.h, p.damping, p.cap_on, p.max_speed);
+        if (more) body_integrate(s.x, s.v, s.xp, i, p.h, gv);
+      }
+      sync();
+    }
+  }
+  if (SMEM) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      g.x[i] = s.x[i];
+      g.v[i] = s.v[i];
+      g.xp[i] = s.xp[i];
+    }
+    for (int j = threadIdx.x; j < m; j += blockDim.x) g.lam[j] = s.lam[j];
+  }
+}
+
+}  // namespace xpbd
+
+// =============================================================================
+// C ABI
+// =============================================================================
+using namespace xpbd;
+
+static Dev3 make_dev3(const xpbd3_state* s) {
+  Dev3 d;
+  d.x = reinterpret_cast<float4*>(s->x);
+  d.v = reinterpret_cast<float4*>(s->v);
+  d.xp = reinterpret_cast<float4*>(s->x_prev);
+  d.acc = reinterpret_cast<float4*>(s->acc);
+  d.lam = s->lam;
+  d.ri = reinterpret_cast<const int4*>(s->row_i);
+  d.rf = reinterpret_cast<const float4*>(s->row_f);
+  d.ra = reinterpret_cast<const float4*>(s->row_anchor);
+  d.n_rows = s->n_rows;
+  d.corder = s->color_order;
+  d.cstarts = s->color_starts;
+  d.n = s->n_bodies;
+  d.ncolors = s->num_colors;
+  return d;
+}
+
+static int check_state(const xpbd3_state* s) {
+  if (!s || s->n_bodies < 0 || !s->x || !s->v || !s->x_prev || !s->n_rows) return XPBD_ERR_BAD_ARG;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_integrate(const xpbd3_state* s, float h, float gx, float gy, float gz, void* stream) {
+  if (check_state(s)) return XPBD_ERR_BAD_ARG;
+  if (s->n_bodies == 0) return XPBD_OK;
+  k3_integrate<<<stream_blocks(s->n_bodies, 256), 256, 0, as_stream(stream)>>>(make_dev3(s), h, gx, gy, gz);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_solve_jacobi(const xpbd3_state* s, float h, int first, void* stream) {
+  if (check_state(s) || !s->acc || !s->row_i) return XPBD_ERR_BAD_ARG;
+  if (s->row_capacity == 0) return XPBD_OK;
+  int blocks = stream_blocks(s->row_capacity, 256);
+  if (first) k3_jacobi<true><<<blocks, 256, 0, as_stream(stream)>>>(make_dev3(s), h);
+  else k3_jacobi<false><<<blocks, 256, 0, as_stream(stream)>>>(make_dev3(s), h);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_apply_jacobi(const xpbd3_state* s, float relax, void* stream) {
+  if (check_state(s) || !s->acc) return XPBD_ERR_BAD_ARG;
+  if (s->n_bodies == 0) return XPBD_OK;
+  k3_apply<<<stream_blocks(s->n_bodies, 256), 256, 0, as_stream(stream)>>>(make_dev3(s), relax);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_solve_color(const xpbd3_state* s, int start, int count, float h, int first,
+                                 void* stream) {
+  if (check_state(s) || !s->color_order || start < 0 || count < 0) return XPBD_ERR_BAD_ARG;
+  if (count == 0) return XPBD_OK;
+  int blocks = stream_blocks(count, 256);
+  if (first) k3_color<true><<<blocks, 256, 0, as_stream(stream)>>>(make_dev3(s), start, count, h);
+  else k3_color<false><<<blocks, 256, 0, as_stream(stream)>>>(make_dev3(s), start, count, h);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_finalize_velocity(const xpbd3_state* s, float h, float damping, void* stream) {
+  if (check_state(s)) return XPBD_ERR_BAD_ARG;
+  if (s->n_bodies == 0) return XPBD_OK;
+  k3_finalize<<<stream_blocks(s->n_bodies, 256), 256, 0, as_stream(stream)>>>(make_dev3(s), h, damping);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_cap_velocity(const xpbd3_state* s, float max_speed, void* stream) {
+  if (check_state(s)) return XPBD_ERR_BAD_ARG;
+  if (s->n_bodies == 0) return XPBD_OK;
+  k3_cap<<<stream_blocks(s->n_bodies, 256), 256, 0, as_stream(stream)>>>(make_dev3(s), max_speed);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+// ---- solver handle -------------------------------------------------------------
+struct xpbd3_solver {
+  xpbd3_state st{};
+  xpbd3_params par{};
+  Dev3 dev{};
+  Par3 p3{};
+  unsigned* bar = nullptr;  // [count, gen, status(int)]
+  int blocks = 1, threads = 256;
+  size_t smem = 0;
+  bool use_smem = false;
+  int force_mode = -1;  // -1 auto, 0 global, 1 shared
+};
+
+static constexpr size_t kSmemMax = 227 * 1024;
+
+template <bool GS, bool SMEM>
+static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream) {
+  GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2)};
+  auto kern = k3_frames<GS, SMEM>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(h->blocks);
+  cfg.blockDim = dim3(h->threads);
+  cfg.dynamicSmemBytes = h->smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = h->blocks > 1 ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  XPBD_CUDA(cudaLaunchKernelEx(&cfg, kern, h->dev, h->p3, frames, gb));
+  return XPBD_OK;
+}
+
+template <bool GS, bool SMEM>
+static int configure(xpbd3_solver* h) {
+  auto kern = k3_frames<GS, SMEM>;
+  if (SMEM) {
+    XPBD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem));
+    h->blocks = 1;
+    return XPBD_OK;
+  }
+  int per_sm = 0;
+  XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, h->threads, 0));
+  if (per_sm < 1) per_sm = 1;
+  long long work = std::max<long long>(h->st.n_bodies, h->st.row_capacity);
+  int want = ceil_div(work, h->threads);
+  h->blocks = std::max(1, std::min(want, per_sm * num_sms()));
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_create(xpbd3_solver** out) {
+  if (!out) return XPBD_ERR_BAD_ARG;
+  xpbd3_solver* h = new xpbd3_solver();
+  cudaError_t e = cudaMalloc(&h->bar, 4 * sizeof(unsigned));
+  if (e != cudaSuccess) {
+    set_last_error("cudaMalloc", e);
+    delete h;
+    return XPBD_ERR_CUDA;
+  }
+  cudaMemset(h->bar, 0, 4 * sizeof(unsigned));
+  *out = h;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_destroy(xpbd3_solver* h) {
+  if (!h) return XPBD_OK;
+  if (h->bar) cudaFree(h->bar);
+  delete h;
+  return XPBD_OK;
+}
+
+// Testing hook: force the frame driver (-1 auto, 0 global memory, 1 shared memory).
+extern "C" int xpbd3_force_mode(xpbd3_solver* h, int mode) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  h->force_mode = mode;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_params* p) {
+  if (!h || check_state(s) || !p) return XPBD_ERR_BAD_ARG;
+  if (p->substeps < 0 || p->iterations < 0) return XPBD_ERR_BAD_ARG;
+  if (p->gs && s->row_capacity > 0 && (!s->color_order || !s->color_starts)) return XPBD_ERR_BAD_ARG;
+  h->st = *s;
+  h->par = *p;
+  h->dev = make_dev3(s);
+  Par3& q = h->p3;
+  q.h = (float)(p->dt / (double)(p->substeps > 0 ? p->substeps : 1));
+  q.gx = p->gravity[0];
+  q.gy = p->gravity[1];
+  q.gz = p->gravity[2];
+  q.damping = p->damping;
+  q.relax = p->jacobi_relax;
+  q.max_speed = p->max_speed;
+  q.cap_on = (p->max_speed > 0.0f && isfinite(p->max_speed)) ? 1 : 0;
+  q.substeps = p->substeps;
+  q.iterations = p->iterations;
+  q.gs = p->gs;
+  size_t smem = (size_t)s->n_bodies * 4 * sizeof(float4) + (size_t)s->row_capacity * sizeof(float);
+  smem = (smem + 15) & ~(size_t)15;
+  bool fits = smem <= kSmemMax;
+  h->use_smem = (h->force_mode == 1) ? fits : (h->force_mode == 0 ? false : fits);
+  if (h->use_smem) {
+    h->smem = smem;
+    long long work = std::max<long long>(s->n_bodies, s->row_capacity / 4);
+    int t = (int)std::min<long long>(1024, std::max<long long>(128, ((work + 31) / 32) * 32));
+    h->threads = t;
+  } else {
+    h->smem = 0;
+    h->threads = 256;
+  }
+  int rc;
+  if (p->gs) rc = h->use_smem ? configure<true, true>(h) : configure<true, false>(h);
+  else rc = h->use_smem ? configure<false, true>(h) : configure<false, false>(h);
+  return rc;
+}
+
+extern "C" int xpbd3_step(xpbd3_solver* h, int frames, void* stream) {
+  if (!h || frames < 0) return XPBD_ERR_BAD_ARG;
+  if (frames == 0 || h->st.n_bodies == 0) return XPBD_OK;
+  cudaStream_t st = as_stream(stream);
+  if (h->par.gs) return h->use_smem ? launch_frames<true, true>(h, frames, st) : launch_frames<true, false>(h, frames, st);
+  return h->use_smem ? launch_frames<false, true>(h, frames, st) : launch_frames<false, false>(h, frames, st);
+}
+
+extern "C" int xpbd3_status(xpbd3_solver* h, int* out, void* stream) {
+  if (!h || !out) return XPBD_ERR_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  XPBD_CUDA(cudaMemcpyAsync(out, h->bar + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+  XPBD_CUDA(cudaStreamSynchronize(st));
+  XPBD_CUDA(cudaMemsetAsync(h->bar + 2, 0, sizeof(int), st));
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int* smem_bytes) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  if (blocks) *blocks = h->blocks;
+  if (threads) *threads = h->threads;
+  if (smem_bytes) *smem_bytes = (int)h->smem;
+  return XPBD_OK;
+}
