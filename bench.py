@@ -36,7 +36,10 @@ WORKLOADS = {
     "spheres": "sphere pile 2048 (16x8x16, r=0.05 m, jitter 0.01, floor + self collision mu=0.5), jacobi 15x2",
     "cloth": "cloth 32x32 (spacing 0.02 m, 0.01 kg, 2 pinned corners, 5826 DISTANCE alpha=1e-8 + 1024 FLOOR mu=0.3), gs 15x2",
     "cloth_jacobi": "cloth 32x32 as above, jacobi 15x2",
+    "boxes": "box pile 1440 (12x10x12 lattice pitch 0.8 m, half extents U[0.1,0.3] m, density 1000, random "
+             "orientation, mu=0.6, e=0.2), LBVH, 15x2",
 }
+SIX_DOF = {"boxes"}
 BYTES_PER_PROJ = {0: 88, 1: 88, 2: 64, 3: 112}   # DISTANCE, ATTACH, FLOOR, CONTACT (Jacobi)
 BYTES_PER_PROJ_GS = {0: 84, 1: 84, 2: 64, 3: 112}
 APPLY_BYTES = 60          # per body per iteration (Jacobi averaged apply)
@@ -48,6 +51,10 @@ def make_solver(workload, device, solver_cls):
     if workload == "spheres":
         s = solver_cls(dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi", device=device)
         scenes.build_sphere_pile(s)
+    elif workload == "boxes":
+        s = solver_cls(dt=1 / 60, substeps=15, iterations=2, floor_y=0.0, friction=0.6, restitution=0.2,
+                       broadphase="lbvh", device=device)
+        scenes.build_box_pile(s)
     elif workload in ("cloth", "cloth_jacobi"):
         mode = "gs" if workload == "cloth" else "jacobi"
         s = solver_cls(dt=1 / 60, substeps=15, iterations=2, solve_mode=mode, device=device)
@@ -135,6 +142,8 @@ def algorithmic_bytes(solver, rows_type_counts, gs):
 
 
 def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
+    if workload in SIX_DOF:
+        return time_engine6(args, workload, device, flush_buf, clocks)
     import ctypes as C
 
     import numpy as np
@@ -198,7 +207,68 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
     return res
 
 
+def time_engine6(args, workload, device, flush_buf, clocks=None):
+    """Box pile: per frame the device broad phase (LBVH build + pair emission)
+    then one persistent launch of all substeps."""
+    import numpy as np
+    import torch
+
+    from xpbd_b200 import Solver6DOF
+    from xpbd_b200 import _native as N
+    from xpbd_b200.solver_6dof import lib6
+
+    s = make_solver(workload, device, Solver6DOF)
+    s.sync_pairs = False
+    s._flush()
+    L = lib6()
+    stream = torch.cuda.current_stream(device)
+    sp = N.stream_of(device)
+    for _ in range(args.warmup):
+        N.check(L.xpbd6_step(s._h, 1, sp))
+    torch.cuda.synchronize(device)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ctx = clocks if clocks is not None else _Null()
+    pts = []
+    with ctx:
+        for k in range(args.steps):
+            if flush_buf is not None:
+                flush_buf.zero_()
+            e0, e1, e2 = ev[k]
+            e0.record(stream)
+            N.check(L.xpbd6_broadphase(s._h, sp))
+            e1.record(stream)
+            N.check(L.xpbd6_substeps(s._h, sp))
+            e2.record(stream)
+        torch.cuda.synchronize(device)
+    frame_ms = [a.elapsed_time(c) for a, _, c in ev]
+    kern_ms = [b.elapsed_time(c) for _, b, c in ev]
+    # graph replay of the whole frame (broad phase + substeps), back to back
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    N.check(L.xpbd6_step(s._h, args.steps, sp))
+    g1.record(stream)
+    torch.cuda.synchronize(device)
+    graph_ms = g0.elapsed_time(g1) / args.steps
+    status = s.status()
+    n = s.num_bodies
+    n_dyn = int((s.tensors["x"][:, 3] > 0).sum().item())
+    npairs = min(s.n_pairs, s.cap)
+    hdr = s.tensors["m_hdr"][:npairs].cpu().numpy()
+    points = int(hdr[:, 0].sum())
+    rows = 8 * n_dyn + points + s.num_joints
+    proj_per_frame = rows * s.substeps * s.iterations
+    S, I = s.substeps, s.iterations
+    alg = S * (I * (points * 196 + 8 * n_dyn * 47 + s.num_joints * 196) + npairs * 300 + n * 128)
+    return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=kern_ms, proj_per_frame=proj_per_frame,
+                rows=rows, bodies=n, status=status, alg_bytes=alg, launches=args.steps * 16, solver=s,
+                launch={"pairs": npairs, "manifold_points": points, "graph_ms_per_frame": round(graph_ms, 5)})
+
+
 def time_e2e(args, workload, device):
+    if workload in SIX_DOF:
+        return time_e2e6(args, workload, device)
     """Same metric through the public API with host buffers: each frame uploads
     the particle state from pinned host memory, steps, and reads the positions
     back into pinned host memory, all inside the CUDA-event-timed region."""
@@ -237,12 +307,53 @@ def time_e2e(args, workload, device):
     return ms, m * s.substeps * s.iterations, h2d, d2h
 
 
+def time_e2e6(args, workload, device):
+    """6-DOF end to end: upload positions/orientations/velocities from pinned
+    host memory, step through the public API (graph replay), read back
+    positions and orientations, inside the timed region."""
+    import torch
+
+    from xpbd_b200 import Solver6DOF
+    s = make_solver(workload, device, Solver6DOF)
+    s.sync_pairs = False
+    s._flush()
+    T = s.tensors
+    keys = ("x", "q", "v", "w")
+    host = {k: T[k].cpu().pin_memory() for k in keys}
+    outx = torch.empty_like(host["x"]).pin_memory()
+    outq = torch.empty_like(host["q"]).pin_memory()
+    stream = torch.cuda.current_stream(device)
+    steps = max(1, args.steps // 2)
+    for _ in range(3):
+        s.step()
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        for k in keys:
+            T[k].copy_(host[k], non_blocking=True)
+        s.step()
+        outx.copy_(T["x"], non_blocking=True)
+        outq.copy_(T["q"], non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1) / steps
+    n_dyn = int((T["x"][:, 3] > 0).sum().item())
+    hdr = T["m_hdr"][:min(s.n_pairs, s.cap)].cpu().numpy()
+    proj = (8 * n_dyn + int(hdr[:, 0].sum()) + s.num_joints) * s.substeps * s.iterations
+    h2d = sum(host[k].numel() * 4 for k in keys)
+    d2h = (outx.numel() + outq.numel()) * 4
+    return ms, proj, h2d, d2h
+
+
 def cpu_baseline(workload, seconds):
     """The oracle (CPU restatement of the reference) on a bounded sample of the
     same workload: consecutive frames from the same initial state until
     `seconds` of host time have elapsed (at least one frame)."""
     from oracle import oracle as O
-    s = make_solver(workload, "cpu", O.OracleSolver)
+    six = workload in SIX_DOF
+    s = make_solver(workload, "cpu", O.OracleSolver6DOF if six else O.OracleSolver)
     s.step()  # first frame outside the sample (builds arrays)
     t0 = time.perf_counter()
     frames = 0
@@ -250,11 +361,20 @@ def cpu_baseline(workload, seconds):
     while True:
         s.step()
         frames += 1
-        proj += s.num_constraints * s.substeps * s.iterations
+        proj += rows_of(s) * s.substeps * s.iterations
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
     return proj / dt / 1e6, frames, dt
+
+
+def rows_of(s):
+    """Projection rows of one substep: all rows (3-DOF, the reference's
+    definition); 8 floor slots per dynamic body + manifold points + joints (6-DOF)."""
+    if hasattr(s, "num_constraints"):
+        return s.num_constraints
+    n_dyn = int((s.inv_mass > 0).sum())
+    return 8 * n_dyn + int(s.m_count[:min(s.n_pairs, s.cap)].sum()) + s.num_joints
 
 
 class _Null:
@@ -271,7 +391,8 @@ def run_reference(args):
         return
     t0 = time.perf_counter()
     from oracle import oracle as O
-    s = make_solver(args.workload, "cpu", O.OracleSolver)
+    six = args.workload in SIX_DOF
+    s = make_solver(args.workload, "cpu", O.OracleSolver6DOF if six else O.OracleSolver)
     for _ in range(args.warmup):
         s.step()
     times = []
@@ -280,7 +401,7 @@ def run_reference(args):
         a = time.perf_counter()
         s.step()
         times.append(time.perf_counter() - a)
-        proj += s.num_constraints * s.substeps * s.iterations
+        proj += rows_of(s) * s.substeps * s.iterations
     total = sum(times)
     value = proj / total / 1e6
     line = {
@@ -349,7 +470,8 @@ def main():
                        "parallelism": f"replicas x{world}", "launch": r["launch"]},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 5), "peak_kind": peak_kind,
-                         "traffic": traffic_for(args.workload), "kernel": "k3_frames (persistent frame kernel)",
+                         "traffic": traffic_for(args.workload),
+                         "kernel": "k6_substeps" if args.workload in SIX_DOF else "k3_frames",
                          "kernel_ms": round(kern_ms, 5), "alg_bytes_per_launch": r["alg_bytes"]},
             "gpu_launches": r["launches"],
             "status_bits": r["status"],

@@ -9,5 +9,7 @@ with the reference's constructor arguments, scene-building calls and
 
 from .scene import Body, ConstraintHandle, Shape
 from .solver import ATTACH, CONTACT, DISTANCE, FLOOR, Solver
+from .solver_6dof import RigidBody, Solver6DOF
 
-__all__ = ["Solver", "Body", "Shape", "ConstraintHandle", "DISTANCE", "ATTACH", "FLOOR", "CONTACT"]
+__all__ = ["Solver", "Solver6DOF", "RigidBody", "Body", "Shape", "ConstraintHandle",
+           "DISTANCE", "ATTACH", "FLOOR", "CONTACT"]

@@ -1,0 +1,1438 @@
+// 6-DOF rigid-body XPBD engine (replaces src/xpbd3d/kernels_6dof.py,
+// kernels_bvh.py and the device part of Solver6DOF.step / _record,
+// solver_6dof.py:357-529).
+//
+// Bodies are float4 records (position + inverse mass, orientation xyzw,
+// velocity, angular velocity, substep-start position/orientation, body-frame
+// inverse inertia, half extents).  Jacobi accumulators are float4 pairs
+// (dx + count, drot) updated with 16-byte vector atomics; each floor body, pair
+// or joint sums its own contributions in registers first and issues one atomic
+// per accumulator and body (the reference issues one per corner / point).
+//
+// One frame = broad phase (separate kernels) + one persistent cooperative
+// launch that runs every substep: phases are separated by a bounded grid
+// barrier, which replaces the reference's ~15 launches per substep.
+#include <algorithm>
+#include <vector>
+
+#include "prims.cuh"
+
+namespace xpbd {
+
+struct Dev6 {
+  float4 *x, *q, *v, *w, *xp, *qp;
+  const float4 *inv_I, *he;
+  const int* group;
+  float4 *ax, *ar, *av, *aw;
+  float* lam_floor;
+  int2* pairs;
+  int* n_pairs;
+  int4* m_hdr;
+  float4* m_normal;
+  float4* m_off_inc;
+  float4* m_off_ref;
+  float* lam_pair;
+  const int2* j_ab;
+  const float4* j_a;  // anchor in A's frame, rest in w
+  const float4* j_b;  // anchor in B's frame, compliance in w
+  float* lam_joint;
+  int n, nj, cap;
+};
+
+struct Par6 {
+  float h, dt, gx, gy, gz, floor_y, mu, rest, lin_damp, ang_damp, relax, max_speed, max_omega, margin;
+  int substeps, iterations, gyro;
+};
+
+XD void vadd(float4* p, V3 d, float c) { red_add4(p, make_float4(d.x, d.y, d.z, c)); }
+
+// ---- kernels_6dof.py:68-102 integrate_bodies (+ the per-substep zeroing of
+// the floor multipliers, solver_6dof.py:374) --------------------------------------
+XD void body_integrate6(const Dev6& s, int i, const Par6& p) {
+  float4 xi = s.x[i], qi = s.q[i];
+  s.xp[i] = xi;
+  s.qp[i] = qi;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) s.lam_floor[8 * i + c] = 0.0f;
+  if (xi.w == 0.0f) return;
+  V3 vi = v3(s.v[i]) + V3{p.gx, p.gy, p.gz} * p.h;
+  s.v[i] = f4(vi, 0.0f);
+  s.x[i] = f4(v3(xi) + vi * p.h, xi.w);
+  Q4 q = q4(qi);
+  V3 wi = v3(s.w[i]);
+  if (p.gyro) {
+    V3 wb = qrot_inv(q, wi);
+    V3 ii = v3(s.inv_I[i]);
+    float ix = ii.x > 0.0f ? 1.0f / ii.x : 0.0f;
+    float iy = ii.y > 0.0f ? 1.0f / ii.y : 0.0f;
+    float iz = ii.z > 0.0f ? 1.0f / ii.z : 0.0f;
+    V3 Iw = V3{ix * wb.x, iy * wb.y, iz * wb.z};
+    V3 tau = -cross(wb, Iw);
+    V3 dwb = V3{ii.x * tau.x, ii.y * tau.y, ii.z * tau.z} * p.h;
+    wi = wi + qrot(q, dwb);
+    s.w[i] = f4(wi, 0.0f);
+  }
+  s.q[i] = f4(quat_integrate(q, wi, p.h));
+}
+
+// ---- kernels_6dof.py:159-211 solve_floor_contacts, one body --------------------------
+XD void floor_body(const Dev6& s, int i, const Par6& p) {
+  float4 x4 = s.x[i];
+  float im = x4.w;
+  if (im == 0.0f) return;
+  V3 xi = v3(x4), he = v3(s.he[i]), Ii = v3(s.inv_I[i]);
+  Q4 qi = q4(s.q[i]);
+  const V3 S = V3{0.0f, 1.0f, 0.0f};
+  V3 dx = V3{0.0f, 0.0f, 0.0f}, dr = V3{0.0f, 0.0f, 0.0f};
+  float cnt = 0.0f;
+  bool any = false;
+  for (int c = 0; c < 8; ++c) {
+    V3 corner = box_corner(he, c);
+    V3 p1 = xi + qrot(qi, corner);
+    float d = p.floor_y - p1.y;
+    int slot = 8 * i + c;
+    if (d <= 0.0f) {
+      s.lam_floor[slot] = 0.0f;
+      continue;
+    }
+    V3 r = p1 - xi;
+    float wg = gen_inv_mass(im, qi, Ii, r, S);
+    if (wg <= 0.0f) continue;
+    float dlam = d / wg;
+    s.lam_floor[slot] = dlam;
+    V3 P = S * dlam;
+    dx = dx + P * im;
+    dr = dr + world_invI_mul(qi, Ii, cross(r, P));
+    cnt += 1.0f;
+    any = true;
+    if (p.mu > 0.0f) {
+      V3 p1b = v3(s.xp[i]) + qrot(q4(s.qp[i]), corner);
+      V3 dp = p1 - p1b;
+      V3 dpt = dp - S * dot(dp, S);
+      float lt = length(dpt);
+      if (lt > kEps && lt < p.mu * d) {
+        float w2 = gen_inv_mass(im, qi, Ii, r, dpt / lt);
+        if (w2 > 0.0f) {
+          V3 pf = (-dpt) / w2;
+          dx = dx + pf * im;
+          dr = dr + world_invI_mul(qi, Ii, cross(r, pf));
+        }
+      }
+    }
+  }
+  if (any) {
+    vadd(s.ax + i, dx, cnt);
+    vadd(s.ar + i, dr, 0.0f);
+  }
+}
+
+// ---- kernels_6dof.py:227-382 generate_box_manifold, one pair ----------------------
+XD float proj_radius(V3 L, const M33& R, V3 e) {
+  return fabsf(e.x * dot(L, mcol(R, 0))) + fabsf(e.y * dot(L, mcol(R, 1))) + fabsf(e.z * dot(L, mcol(R, 2)));
+}
+
+XD void manifold_pair(const Dev6& s, int pid, float margin) {
+  int4 hdr = make_int4(0, 0, 0, 0);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) s.lam_pair[8 * pid + c] = 0.0f;
+  int2 pr = s.pairs[pid];
+  const int a = pr.x, b = pr.y;
+  V3 cA = v3(s.x[a]), cB = v3(s.x[b]), eA = v3(s.he[a]), eB = v3(s.he[b]);
+  M33 RA = q2m(q4(s.q[a])), RB = q2m(q4(s.q[b]));
+  V3 cBA = cA - cB;
+  float best_overlap = 1.0e30f;
+  V3 best_axis = V3{0.0f, 1.0f, 0.0f};
+  int ref_is_a = 1, best_k = 0;
+  for (int k = 0; k < 3; ++k) {
+    V3 L = mcol(RA, k);
+    float ov = comp(eA, k) + proj_radius(L, RB, eB) - fabsf(dot(L, cBA));
+    if (ov < 0.0f) { s.m_hdr[pid] = hdr; return; }
+    if (ov < best_overlap) { best_overlap = ov; best_axis = L; ref_is_a = 1; best_k = k; }
+  }
+  for (int k = 0; k < 3; ++k) {
+    V3 L = mcol(RB, k);
+    float ov = comp(eB, k) + proj_radius(L, RA, eA) - fabsf(dot(L, cBA));
+    if (ov < 0.0f) { s.m_hdr[pid] = hdr; return; }
+    if (ov < best_overlap) { best_overlap = ov; best_axis = L; ref_is_a = 0; best_k = k; }
+  }
+  V3 nBA = best_axis;
+  if (dot(nBA, cBA) < 0.0f) nBA = -nBA;
+  int ref_b, inc_b;
+  V3 c_ref, e_ref, c_inc, e_inc, ref_face_n;
+  M33 R_ref, R_inc;
+  if (ref_is_a) {
+    ref_b = a; inc_b = b; c_ref = cA; R_ref = RA; e_ref = eA; c_inc = cB; R_inc = RB; e_inc = eB;
+    ref_face_n = -nBA;
+  } else {
+    ref_b = b; inc_b = a; c_ref = cB; R_ref = RB; e_ref = eB; c_inc = cA; R_inc = RA; e_inc = eA;
+    ref_face_n = nBA;
+  }
+  const int ref_axis = best_k;
+  V3 ref_face_c = c_ref + ref_face_n * comp(e_ref, ref_axis);
+  int ax1 = (ref_axis + 1) % 3, ax2 = (ref_axis + 2) % 3;
+  V3 u_ref = mcol(R_ref, ax1), v_ref = mcol(R_ref, ax2);
+  float eu = comp(e_ref, ax1), ev = comp(e_ref, ax2);
+  int inc_axis = 0;
+  float inc_sign = 1.0f, best_dot = -1.0e30f;
+  for (int k = 0; k < 3; ++k) {
+    V3 col = mcol(R_inc, k);
+    float dp = -dot(col, ref_face_n);
+    if (dp > best_dot) { best_dot = dp; inc_axis = k; inc_sign = 1.0f; }
+    if (-dp > best_dot) { best_dot = -dp; inc_axis = k; inc_sign = -1.0f; }
+  }
+  V3 inc_n = mcol(R_inc, inc_axis) * inc_sign;
+  V3 inc_face_c = c_inc + inc_n * comp(e_inc, inc_axis);
+  int iax1 = (inc_axis + 1) % 3, iax2 = (inc_axis + 2) % 3;
+  V3 iu = mcol(R_inc, iax1), iv = mcol(R_inc, iax2);
+  float ieu = comp(e_inc, iax1), iev = comp(e_inc, iax2);
+  V3 poly[16];
+  int cur = 0, nxt = 8;
+  poly[0] = (inc_face_c + iu * ieu) + iv * iev;
+  poly[1] = (inc_face_c - iu * ieu) + iv * iev;
+  poly[2] = (inc_face_c - iu * ieu) - iv * iev;
+  poly[3] = (inc_face_c + iu * ieu) - iv * iev;
+  int plen = 4;
+  for (int pi = 0; pi < 4; ++pi) {
+    V3 pp, pn;
+    if (pi == 0) { pp = ref_face_c + u_ref * eu; pn = u_ref; }
+    else if (pi == 1) { pp = ref_face_c - u_ref * eu; pn = -u_ref; }
+    else if (pi == 2) { pp = ref_face_c + v_ref * ev; pn = v_ref; }
+    else { pp = ref_face_c - v_ref * ev; pn = -v_ref; }
+    if (plen == 0) { s.m_hdr[pid] = hdr; return; }
+    int olen = 0;
+    for (int k = 0; k < plen; ++k) {
+      V3 ap = poly[cur + k], bp = poly[cur + (k + 1) % plen];
+      float da = dot(ap - pp, pn), db = dot(bp - pp, pn);
+      if (da <= 0.0f) {
+        if (olen < 8) poly[nxt + olen++] = ap;
+        if (db > 0.0f) {
+          float t = da / (da - db);
+          if (olen < 8) poly[nxt + olen++] = ap + (bp - ap) * t;
+        }
+      } else if (db <= 0.0f) {
+        float t = da / (da - db);
+        if (olen < 8) poly[nxt + olen++] = ap + (bp - ap) * t;
+      }
+    }
+    int tmp = cur; cur = nxt; nxt = tmp;
+    plen = olen;
+  }
+  int nc = 0;
+  for (int k = 0; k < plen; ++k) {
+    if (nc >= 8) break;
+    V3 p_inc = poly[cur + k];
+    float d_signed = dot(p_inc - ref_face_c, ref_face_n);
+    if (d_signed < margin) {
+      V3 p_ref = p_inc - ref_face_n * d_signed;
+      s.m_off_inc[8 * pid + nc] = f4(mtv(R_inc, p_inc - c_inc), 0.0f);
+      s.m_off_ref[8 * pid + nc] = f4(mtv(R_ref, p_ref - c_ref), 0.0f);
+      ++nc;
+    }
+  }
+  hdr = make_int4(nc, inc_b, ref_b, 0);
+  s.m_hdr[pid] = hdr;
+  s.m_normal[pid] = f4(ref_face_n, 0.0f);
+}
+
+// ---- kernels_6dof.py:386-430 solve_box_manifold, one pair -------------------------
+XD void box_pair(const Dev6& s, int pid) {
+  int4 hdr = s.m_hdr[pid];
+  const int nc = hdr.x;
+  if (nc == 0) return;
+  const int inc = hdr.y, ref = hdr.z;
+  V3 S = v3(s.m_normal[pid]);
+  float4 xi4 = s.x[inc], xr4 = s.x[ref];
+  V3 xi = v3(xi4), xr = v3(xr4);
+  Q4 qi = q4(s.q[inc]), qr = q4(s.q[ref]);
+  V3 Ii = v3(s.inv_I[inc]), Ir = v3(s.inv_I[ref]);
+  const float imi = xi4.w, imr = xr4.w;
+  V3 dxi = V3{0, 0, 0}, dri = V3{0, 0, 0}, dxr = V3{0, 0, 0}, drr = V3{0, 0, 0};
+  float ci = 0.0f, cr = 0.0f;
+  for (int c = 0; c < nc; ++c) {
+    int slot = 8 * pid + c;
+    V3 p_inc = xi + qrot(qi, v3(s.m_off_inc[slot]));
+    V3 p_ref = xr + qrot(qr, v3(s.m_off_ref[slot]));
+    float C = dot(p_inc - p_ref, S);
+    if (C >= 0.0f) {
+      s.lam_pair[slot] = 0.0f;
+      continue;
+    }
+    float d = -C;
+    V3 r_inc = p_inc - xi, r_ref = p_ref - xr;
+    float w_inc = gen_inv_mass(imi, qi, Ii, r_inc, S);
+    float w_ref = gen_inv_mass(imr, qr, Ir, r_ref, S);
+    float wsum = w_inc + w_ref;
+    if (wsum <= 0.0f) continue;
+    float dlam = d / wsum;
+    s.lam_pair[slot] = s.lam_pair[slot] + dlam;
+    V3 P = S * dlam;
+    if (imi > 0.0f) {
+      dxi = dxi + P * imi;
+      dri = dri + world_invI_mul(qi, Ii, cross(r_inc, P));
+      ci += 1.0f;
+    }
+    if (imr > 0.0f) {
+      dxr = dxr + (-P) * imr;
+      drr = drr + (-world_invI_mul(qr, Ir, cross(r_ref, P)));
+      cr += 1.0f;
+    }
+  }
+  if (ci > 0.0f) {
+    vadd(s.ax + inc, dxi, ci);
+    vadd(s.ar + inc, dri, 0.0f);
+  }
+  if (cr > 0.0f) {
+    vadd(s.ax + ref, dxr, cr);
+    vadd(s.ar + ref, drr, 0.0f);
+  }
+}
+
+// ---- kernels_6dof.py:441-483 solve_joints, one joint --------------------------------
+XD void joint_row(const Dev6& s, int k, float h) {
+  int2 ab = s.j_ab[k];
+  const int a = ab.x, b = ab.y;
+  float4 xa4 = s.x[a], xb4 = s.x[b], ja = s.j_a[k], jb = s.j_b[k];
+  V3 xa = v3(xa4), xb = v3(xb4);
+  Q4 qa = q4(s.q[a]), qb = q4(s.q[b]);
+  V3 pa = xa + qrot(qa, v3(ja));
+  V3 pb = xb + qrot(qb, v3(jb));
+  V3 d = pa - pb;
+  float dist = length(d);
+  if (dist < kEps) return;
+  V3 n = d / dist;
+  float C = dist - ja.w;
+  V3 ra = pa - xa, rb = pb - xb;
+  V3 Ia = v3(s.inv_I[a]), Ib = v3(s.inv_I[b]);
+  float wa = gen_inv_mass(xa4.w, qa, Ia, ra, n);
+  float wb = gen_inv_mass(xb4.w, qb, Ib, rb, n);
+  float wsum = wa + wb;
+  if (wsum <= 0.0f) return;
+  float alpha = jb.w / (h * h);
+  float lam = s.lam_joint[k];
+  float dlam = (-C - alpha * lam) / (wsum + alpha);
+  s.lam_joint[k] = lam + dlam;
+  V3 P = n * dlam;
+  if (xa4.w > 0.0f) {
+    vadd(s.ax + a, P * xa4.w, 1.0f);
+    vadd(s.ar + a, world_invI_mul(qa, Ia, cross(ra, P)), 0.0f);
+  }
+  if (b >= 0 && xb4.w > 0.0f) {
+    vadd(s.ax + b, (-P) * xb4.w, 1.0f);
+    vadd(s.ar + b, -world_invI_mul(qb, Ib, cross(rb, P)), 0.0f);
+  }
+}
+
+// ---- kernels_6dof.py:487-535 apply_jacobi_6dof + finalize_velocity_6dof --------------
+XD void body_apply6(const Dev6& s, int i, float relax) {
+  float4 a = s.ax[i];
+  int n = (int)a.w;
+  float4 x4 = s.x[i];
+  if (n > 0 && x4.w > 0.0f) {
+    float inv_n = relax / (float)n;
+    s.x[i] = f4(v3(x4) + v3(a) * inv_n, x4.w);
+    V3 dw = v3(s.ar[i]) * inv_n;
+    Q4 qi = q4(s.q[i]);
+    Q4 pq = qmul(Q4{dw.x, dw.y, dw.z, 0.0f}, qi);
+    s.q[i] = f4(qnormalize(Q4{qi.x + 0.5f * pq.x, qi.y + 0.5f * pq.y, qi.z + 0.5f * pq.z, qi.w + 0.5f * pq.w}));
+  }
+  s.ax[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  s.ar[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+XD void body_finalize6(const Dev6& s, int i, const Par6& p) {
+  float4 x4 = s.x[i];
+  if (x4.w == 0.0f) {
+    s.v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    s.w[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    return;
+  }
+  s.v[i] = f4(((v3(x4) - v3(s.xp[i])) / p.h) * (1.0f - p.lin_damp), 0.0f);
+  Q4 dq = qmul(q4(s.q[i]), qconj(q4(s.qp[i])));
+  V3 w = V3{dq.x, dq.y, dq.z} * (2.0f / p.h);
+  if (dq.w < 0.0f) w = -w;
+  s.w[i] = f4(w * (1.0f - p.ang_damp), 0.0f);
+}
+
+// ---- kernels_6dof.py:542-659 velocity_floor / velocity_box --------------------------
+XD V3 velocity_impulse(V3 vrel, V3 S, float lam_n, const Par6& p) {
+  float vn = dot(vrel, S);
+  V3 vt = vrel - S * vn;
+  float ltan = length(vt);
+  V3 impulse = V3{0.0f, 0.0f, 0.0f};
+  if (p.mu > 0.0f && ltan > kEps) {
+    float fn = lam_n / (p.h * p.h);
+    float dvm = fmin_r(p.h * p.mu * fabsf(fn), ltan);
+    impulse = impulse - (vt / ltan) * dvm;
+  }
+  if (vn < 0.0f) impulse = impulse + S * (-vn + fmax_r(-p.rest * vn, 0.0f));
+  return impulse;
+}
+
+XD void velocity_floor_body(const Dev6& s, int i, const Par6& p) {
+  float4 x4 = s.x[i];
+  float im = x4.w;
+  if (im == 0.0f) return;
+  const V3 S = V3{0.0f, 1.0f, 0.0f};
+  Q4 qi = q4(s.q[i]);
+  V3 Ii = v3(s.inv_I[i]), he = v3(s.he[i]), vi = v3(s.v[i]), wi = v3(s.w[i]);
+  V3 dv = V3{0, 0, 0}, dw = V3{0, 0, 0};
+  float cnt = 0.0f;
+  for (int c = 0; c < 8; ++c) {
+    float lam_n = s.lam_floor[8 * i + c];
+    if (lam_n == 0.0f) continue;
+    V3 r = qrot(qi, box_corner(he, c));
+    V3 vc = vi + cross(wi, r);
+    V3 impulse = velocity_impulse(vc, S, lam_n, p);
+    if (length(impulse) > kEps) {
+      float wg = gen_inv_mass(im, qi, Ii, r, impulse / length(impulse));
+      if (wg > 0.0f) {
+        V3 P = impulse / wg;
+        dv = dv + P * im;
+        dw = dw + world_invI_mul(qi, Ii, cross(r, P));
+        cnt += 1.0f;
+      }
+    }
+  }
+  if (cnt > 0.0f) {
+    vadd(s.av + i, dv, cnt);
+    vadd(s.aw + i, dw, 0.0f);
+  }
+}
+
+XD void velocity_box_pair(const Dev6& s, int pid, const Par6& p) {
+  int4 hdr = s.m_hdr[pid];
+  const int nc = hdr.x;
+  if (nc == 0) return;
+  const int ci = hdr.y, cj = hdr.z;
+  V3 S = v3(s.m_normal[pid]);
+  float4 xi4 = s.x[ci], xj4 = s.x[cj];
+  V3 xi = v3(xi4), xj = v3(xj4);
+  Q4 qi = q4(s.q[ci]), qj = q4(s.q[cj]);
+  V3 Ii = v3(s.inv_I[ci]), Ij = v3(s.inv_I[cj]);
+  V3 vi = v3(s.v[ci]), vj = v3(s.v[cj]), wi = v3(s.w[ci]), wj = v3(s.w[cj]);
+  const float imi = xi4.w, imj = xj4.w;
+  V3 dvi = V3{0, 0, 0}, dwi = V3{0, 0, 0}, dvj = V3{0, 0, 0}, dwj = V3{0, 0, 0};
+  float ni = 0.0f, nj = 0.0f;
+  for (int c = 0; c < nc; ++c) {
+    int slot = 8 * pid + c;
+    float lam_n = s.lam_pair[slot];
+    if (lam_n == 0.0f) continue;
+    V3 p_inc = xi + qrot(qi, v3(s.m_off_inc[slot]));
+    V3 p_ref = xj + qrot(qj, v3(s.m_off_ref[slot]));
+    V3 ri = p_inc - xi, rj = p_ref - xj;
+    V3 vrel = (vi + cross(wi, ri)) - (vj + cross(wj, rj));
+    V3 impulse = velocity_impulse(vrel, S, lam_n, p);
+    float li = length(impulse);
+    if (li > kEps) {
+      V3 ndir = impulse / li;
+      float wgi = gen_inv_mass(imi, qi, Ii, ri, ndir);
+      float wgj = gen_inv_mass(imj, qj, Ij, rj, ndir);
+      float wsum = wgi + wgj;
+      if (wsum > 0.0f) {
+        V3 P = impulse / wsum;
+        if (imi > 0.0f) {
+          dvi = dvi + P * imi;
+          dwi = dwi + world_invI_mul(qi, Ii, cross(ri, P));
+          ni += 1.0f;
+        }
+        if (imj > 0.0f) {
+          dvj = dvj + (-P) * imj;
+          dwj = dwj + (-world_invI_mul(qj, Ij, cross(rj, P)));
+          nj += 1.0f;
+        }
+      }
+    }
+  }
+  if (ni > 0.0f) {
+    vadd(s.av + ci, dvi, ni);
+    vadd(s.aw + ci, dwi, 0.0f);
+  }
+  if (nj > 0.0f) {
+    vadd(s.av + cj, dvj, nj);
+    vadd(s.aw + cj, dwj, 0.0f);
+  }
+}
+
+// ---- kernels_6dof.py:663-691 apply_velocity_6dof + cap_velocity_6dof -----------------
+XD void body_apply_velocity6(const Dev6& s, int i, const Par6& p) {
+  float4 a = s.av[i];
+  int n = (int)a.w;
+  V3 vi = v3(s.v[i]), wi = v3(s.w[i]);
+  if (n > 0 && s.x[i].w > 0.0f) {
+    float inv_n = 1.0f / (float)n;
+    vi = vi + v3(a) * inv_n;
+    wi = wi + v3(s.aw[i]) * inv_n;
+  }
+  s.av[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  s.aw[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (p.max_speed > 0.0f) {
+    float sp = length(vi);
+    if (sp > p.max_speed) vi = vi * (p.max_speed / sp);
+    float sa = length(wi);
+    if (p.max_omega > 0.0f && sa > p.max_omega) wi = wi * (p.max_omega / sa);
+  }
+  s.v[i] = f4(vi, 0.0f);
+  s.w[i] = f4(wi, 0.0f);
+}
+
+// ---------------------------------------------------------------------------------
+// Persistent substep kernel: every substep of one frame in one launch.
+__global__ void __launch_bounds__(256) k6_substeps(Dev6 s, Par6 p, GridBarrier bar) {
+  const int n = s.n, nj = s.nj;
+  const int np = min(*s.n_pairs, s.cap);
+  const int t0 = gtid(), st = gstride();
+  const int nb = max(n, nj);
+  for (int i = t0; i < nb; i += st) {
+    if (i < n) body_integrate6(s, i, p);
+    if (i < nj) s.lam_joint[i] = 0.0f;
+  }
+  grid_sync(bar);
+  for (int sub = 0; sub < p.substeps; ++sub) {
+    const bool more = sub + 1 < p.substeps;
+    for (int pid = t0; pid < np; pid += st) manifold_pair(s, pid, p.margin);
+    grid_sync(bar);
+    for (int it = 0; it < p.iterations; ++it) {
+      const int work = nj + n + np;
+      for (int t = t0; t < work; t += st) {
+        if (t < nj) joint_row(s, t, p.h);
+        else if (t < nj + n) floor_body(s, t - nj, p);
+        else box_pair(s, t - nj - n);
+      }
+      grid_sync(bar);
+      const bool last = it + 1 == p.iterations;
+      for (int i = t0; i < n; i += st) {
+        body_apply6(s, i, p.relax);
+        if (last) body_finalize6(s, i, p);
+      }
+      grid_sync(bar);
+    }
+    if (p.iterations == 0) {
+      for (int i = t0; i < n; i += st) body_finalize6(s, i, p);
+      grid_sync(bar);
+    }
+    for (int t = t0; t < n + np; t += st) {
+      if (t < n) velocity_floor_body(s, t, p);
+      else velocity_box_pair(s, t - n, p);
+    }
+    grid_sync(bar);
+    for (int i = t0; i < nb; i += st) {
+      if (i < n) {
+        body_apply_velocity6(s, i, p);
+        if (more) body_integrate6(s, i, p);
+      }
+      if (more && i < nj) s.lam_joint[i] = 0.0f;
+    }
+    grid_sync(bar);
+  }
+}
+
+// per-kernel entry points (parity tests)
+__global__ void k6_integrate(Dev6 s, Par6 p) {
+  for (int i = gtid(); i < max(s.n, s.nj); i += gstride()) {
+    if (i < s.n) body_integrate6(s, i, p);
+    if (i < s.nj) s.lam_joint[i] = 0.0f;
+  }
+}
+__global__ void k6_manifold(Dev6 s, float margin) {
+  const int np = min(*s.n_pairs, s.cap);
+  for (int pid = gtid(); pid < np; pid += gstride()) manifold_pair(s, pid, margin);
+}
+__global__ void k6_solve_positions(Dev6 s, Par6 p) {
+  const int np = min(*s.n_pairs, s.cap);
+  const int work = s.nj + s.n + np;
+  for (int t = gtid(); t < work; t += gstride()) {
+    if (t < s.nj) joint_row(s, t, p.h);
+    else if (t < s.nj + s.n) floor_body(s, t - s.nj, p);
+    else box_pair(s, t - s.nj - s.n);
+  }
+}
+__global__ void k6_apply(Dev6 s, float relax) {
+  for (int i = gtid(); i < s.n; i += gstride()) body_apply6(s, i, relax);
+}
+__global__ void k6_finalize(Dev6 s, Par6 p) {
+  for (int i = gtid(); i < s.n; i += gstride()) body_finalize6(s, i, p);
+}
+__global__ void k6_solve_velocities(Dev6 s, Par6 p) {
+  const int np = min(*s.n_pairs, s.cap);
+  for (int t = gtid(); t < s.n + np; t += gstride()) {
+    if (t < s.n) velocity_floor_body(s, t, p);
+    else velocity_box_pair(s, t - s.n, p);
+  }
+}
+__global__ void k6_apply_velocity(Dev6 s, Par6 p) {
+  for (int i = gtid(); i < s.n; i += gstride()) body_apply_velocity6(s, i, p);
+}
+
+// =================================================================================
+// LBVH broad phase (kernels_bvh.py + wp.Bvh(constructor="lbvh") + emit_pairs)
+// =================================================================================
+struct BP6 {
+  float4* lo;          // n: inflated body AABB lower
+  float4* hi;          // n: upper
+  int* bounds;         // 6: ordered-int min xyz, max xyz of AABB centres
+  uint64_t* keys;      // n
+  uint32_t* vals;      // n
+  void* sort_tmp;
+  int2* child;         // n-1 internal nodes
+  int* parent;         // 2n-1
+  float4* nlo;         // 2n-1
+  float4* nhi;         // 2n-1
+  int* flags;          // n-1
+  int* counts;         // n (or 14 n for grid)
+  int* offsets;
+  void* scan_tmp;
+  // hashgrid / grid
+  int4* cell;          // n
+  uint64_t* ckey;      // n sorted cell keys
+  uint32_t* cval;      // n
+  int* red;            // 16 ints of reductions
+  float4* half;        // n world AABB half extents (grid)
+};
+
+XD int ord_f(float f) {
+  int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+XD float unord_f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+__global__ void k6_bp_init(BP6 b) {
+  if (threadIdx.x < 3) {
+    b.bounds[threadIdx.x] = 0x7fffffff;
+    b.bounds[3 + threadIdx.x] = (int)0x80000000;
+  }
+}
+
+// kernels_bvh.py:22-48 compute_body_aabb (+ centre bounds for the Morton keys)
+XD void body_aabb(const Dev6& s, int i, float man_margin, float dt, float4* lo, float4* hi) {
+  M33 R = q2m(q4(s.q[i]));
+  V3 e = v3(s.he[i]);
+  float ax = fabsf(R.m[0][0]) * e.x + fabsf(R.m[0][1]) * e.y + fabsf(R.m[0][2]) * e.z;
+  float ay = fabsf(R.m[1][0]) * e.x + fabsf(R.m[1][1]) * e.y + fabsf(R.m[1][2]) * e.z;
+  float az = fabsf(R.m[2][0]) * e.x + fabsf(R.m[2][1]) * e.y + fabsf(R.m[2][2]) * e.z;
+  V3 half = V3{ax, ay, az};
+  float rr = length(e);
+  float m = man_margin + dt * (length(v3(s.v[i])) + length(v3(s.w[i])) * rr);
+  V3 pad = V3{m, m, m};
+  V3 xi = v3(s.x[i]);
+  lo[i] = f4((xi - half) - pad, 0.0f);
+  hi[i] = f4((xi + half) + pad, 0.0f);
+}
+
+__global__ void k6_aabb(Dev6 s, Par6 p, BP6 b) {
+  int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    body_aabb(s, i, p.margin, p.dt, b.lo, b.hi);
+    float4 l = b.lo[i], h = b.hi[i];
+    float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+    for (int d = 0; d < 3; ++d) {
+      lmin[d] = min(lmin[d], ord_f(c[d]));
+      lmax[d] = max(lmax[d], ord_f(c[d]));
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o; o >>= 1) {
+      lmin[d] = min(lmin[d], __shfl_xor_sync(0xffffffffu, lmin[d], o));
+      lmax[d] = max(lmax[d], __shfl_xor_sync(0xffffffffu, lmax[d], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&b.bounds[d], lmin[d]);
+      atomicMax(&b.bounds[3 + d], lmax[d]);
+    }
+  }
+}
+
+XD uint32_t expand10(uint32_t v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+XD uint32_t quant10(float t) {
+  float sc = t * 1024.0f;
+  if (!(sc > 0.0f)) sc = 0.0f;
+  if (sc > 1023.0f) sc = 1023.0f;
+  return (uint32_t)sc;
+}
+
+// The LBVH key: AABB centre normalised to the bounds of all centres, 10 bits
+// per axis, interleaved x-major.  Same definition as the oracle's
+// or_morton_codes.
+__global__ void k6_morton(int n, BP6 b) {
+  float cmin[3], inv[3];
+  for (int d = 0; d < 3; ++d) {
+    cmin[d] = unord_f(b.bounds[d]);
+    float ext = unord_f(b.bounds[3 + d]) - cmin[d];
+    inv[d] = ext > 0.0f ? 1.0f / ext : 0.0f;
+  }
+  for (int i = gtid(); i < n; i += gstride()) {
+    float4 l = b.lo[i], h = b.hi[i];
+    float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+    uint32_t k = 0;
+    for (int d = 0; d < 3; ++d) k |= expand10(quant10((c[d] - cmin[d]) * inv[d])) << (2 - d);
+    b.keys[i] = k;
+    b.vals[i] = (uint32_t)i;
+  }
+}
+
+XD int lbvh_delta(const uint64_t* k, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  uint32_t a = (uint32_t)k[i], c = (uint32_t)k[j];
+  if (a == c) return 32 + __clz(i ^ j);
+  return __clz(a ^ c);
+}
+
+// Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees
+// and k-d trees", Algorithm 3: internal node i of the radix tree over sorted
+// keys (duplicates broken by index).  Internal nodes 0..n-2, leaf k = n-1+k.
+__global__ void k6_build(int n, BP6 b) {
+  for (int i = gtid(); i < n - 1; i += gstride()) {
+    const uint64_t* k = b.keys;
+    int d = (lbvh_delta(k, n, i, i + 1) - lbvh_delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = lbvh_delta(k, n, i, i - d);
+    int lmax = 2;
+    while (lbvh_delta(k, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+      if (lbvh_delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = lbvh_delta(k, n, i, j);
+    int s = 0;
+    for (int div = 2;; div *= 2) {
+      int t = (l + div - 1) / div;
+      if (lbvh_delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+      if (t <= 1) break;
+    }
+    int gamma = i + s * d + min(d, 0);
+    int left = (min(i, j) == gamma) ? (n - 1 + gamma) : gamma;
+    int right = (max(i, j) == gamma + 1) ? (n - 1 + gamma + 1) : gamma + 1;
+    b.child[i] = make_int2(left, right);
+    b.parent[left] = i;
+    b.parent[right] = i;
+    b.flags[i] = 0;
+    if (i == 0) b.parent[0] = -1;
+  }
+}
+
+// Bottom-up bounds: the second child to arrive at a node writes its union.
+__global__ void k6_refit(int n, BP6 b) {
+  for (int k = gtid(); k < n; k += gstride()) {
+    int node = n - 1 + k;
+    int body = (int)b.vals[k];
+    b.nlo[node] = b.lo[body];
+    b.nhi[node] = b.hi[body];
+    __threadfence();
+    int cur = b.parent[node];
+    while (cur >= 0) {
+      if (atomicAdd(&b.flags[cur], 1) == 0) break;
+      __threadfence();
+      int2 c = b.child[cur];
+      float4 l0 = __ldcg(b.nlo + c.x), l1 = __ldcg(b.nlo + c.y);
+      float4 h0 = __ldcg(b.nhi + c.x), h1 = __ldcg(b.nhi + c.y);
+      b.nlo[cur] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
+      b.nhi[cur] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
+      __threadfence();
+      cur = b.parent[cur];
+    }
+  }
+}
+
+XD bool overlaps(float4 alo, float4 ahi, float4 blo, float4 bhi) {
+  return blo.x <= ahi.x && blo.y <= ahi.y && blo.z <= ahi.z && bhi.x >= alo.x && bhi.y >= alo.y && bhi.z >= alo.z;
+}
+
+XD bool keep_pair(const Dev6& s, int i, int j) {
+  if (!(j > i)) return false;
+  if (s.x[i].w == 0.0f && s.x[j].w == 0.0f) return false;
+  int gi = s.group[i];
+  if (gi == s.group[j] && gi > 0) return false;
+  return true;
+}
+
+constexpr int kStack = 64;
+
+// kernels_bvh.py:52-85 emit_pairs: tree query of body i's box.  `emit(j)` per kept pair.
+template <class Emit>
+XD void lbvh_query(const Dev6& s, const BP6& b, int i, int* status, Emit emit) {
+  const int n = s.n;
+  if (n < 2) return;
+  float4 qlo = b.lo[i], qhi = b.hi[i];
+  int stack[kStack];
+  int sp = 0;
+  int node = 0;
+  while (true) {
+    int2 c = b.child[node];
+    int ch[2] = {c.x, c.y};
+    for (int e = 0; e < 2; ++e) {
+      int x = ch[e];
+      if (!overlaps(qlo, qhi, b.nlo[x], b.nhi[x])) continue;
+      if (x >= n - 1) {
+        int j = (int)b.vals[x - (n - 1)];
+        if (keep_pair(s, i, j)) emit(j);
+      } else if (sp < kStack) {
+        stack[sp++] = x;
+      } else {
+        raise_status(status, XPBD_ERR_OVERFLOW);
+      }
+    }
+    if (sp == 0) break;
+    node = stack[--sp];
+  }
+}
+
+__global__ void k6_pairs_count(Dev6 s, BP6 b, int* status) {
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    int cnt = 0;
+    lbvh_query(s, b, i, status, [&](int) { ++cnt; });
+    b.counts[i] = cnt;
+  }
+}
+
+// Writes body i's pairs at its scan offset, then sorts its segment by j so the
+// list is ordered by (i, j) whatever the traversal order.
+XD void sort_segment(int2* pairs, int lo, int hi) {
+  for (int a = lo + 1; a < hi; ++a) {
+    int2 key = pairs[a];
+    int b2 = a - 1;
+    while (b2 >= lo && pairs[b2].y > key.y) {
+      pairs[b2 + 1] = pairs[b2];
+      --b2;
+    }
+    pairs[b2 + 1] = key;
+  }
+}
+
+__global__ void k6_pairs_write(Dev6 s, BP6 b, int* status) {
+  const int total = *s.n_pairs;
+  if (gtid() == 0 && total > s.cap) raise_status(status, XPBD_ERR_OVERFLOW);
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    if (b.counts[i] == 0) continue;
+    const int base = b.offsets[i];
+    int r = 0;
+    lbvh_query(s, b, i, status, [&](int j) {
+      if (base + r < s.cap) s.pairs[base + r] = make_int2(i, j);
+      ++r;
+    });
+    sort_segment(s.pairs, base, min(base + r, s.cap));
+  }
+}
+
+// =================================================================================
+// Hash-grid broad phase (kernels_hashgrid.py:122-173 over wp.HashGrid): for body
+// i, the bodies whose cell floor(x/cell) lies in floor((x_i -+ qr)/cell) on
+// every axis, j > i, passing the per-axis inflated-box test.
+// =================================================================================
+__global__ void k6_hg_cells(Dev6 s, Par6 p, BP6 b, float cell) {
+  int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    float4 x = s.x[i];
+    int c[3] = {(int)floorf(x.x / cell), (int)floorf(x.y / cell), (int)floorf(x.z / cell)};
+    b.cell[i] = make_int4(c[0], c[1], c[2], 0);
+    for (int d = 0; d < 3; ++d) {
+      lmin[d] = min(lmin[d], c[d]);
+      lmax[d] = max(lmax[d], c[d]);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o; o >>= 1) {
+      lmin[d] = min(lmin[d], __shfl_xor_sync(0xffffffffu, lmin[d], o));
+      lmax[d] = max(lmax[d], __shfl_xor_sync(0xffffffffu, lmax[d], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&b.red[d], lmin[d]);
+      atomicMax(&b.red[3 + d], lmax[d]);
+    }
+  }
+}
+
+__global__ void k6_red_init(BP6 b) {
+  if (threadIdx.x < 3) {
+    b.red[threadIdx.x] = 0x7fffffff;
+    b.red[3 + threadIdx.x] = (int)0x80000000;
+  }
+  if (threadIdx.x >= 6 && threadIdx.x < 16) b.red[threadIdx.x] = 0;
+}
+
+XD uint64_t cell_key(const int* red, int cx, int cy, int cz) {
+  uint64_t ex = (uint64_t)(red[3] - red[0] + 1), ey = (uint64_t)(red[4] - red[1] + 1);
+  (void)ex;
+  uint64_t ez = (uint64_t)(red[5] - red[2] + 1);
+  return ((uint64_t)(cx - red[0]) * ey + (uint64_t)(cy - red[1])) * ez + (uint64_t)(cz - red[2]);
+}
+
+__global__ void k6_hg_keys(int n, BP6 b) {
+  for (int i = gtid(); i < n; i += gstride()) {
+    int4 c = b.cell[i];
+    b.ckey[i] = cell_key(b.red, c.x, c.y, c.z);
+    b.cval[i] = (uint32_t)i;
+  }
+}
+
+XD int lower_bound_key(const uint64_t* a, int n, uint64_t t) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] < t) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+template <class Emit>
+XD void hg_query(const Dev6& s, const BP6& b, int i, float man_margin, float dt, float rs_max, float cell,
+                 Emit emit) {
+  V3 e_i = v3(s.he[i]);
+  float rs_i = length(e_i);
+  float mi = fmin_r(dt * (length(v3(s.v[i])) + length(v3(s.w[i])) * rs_i), rs_i);
+  float qr = fmin_r(rs_i + rs_max + man_margin + mi, cell);
+  V3 half_i = aabb_half(q4(s.q[i]), e_i);
+  V3 xi = v3(s.x[i]);
+  int lo[3] = {(int)floorf((xi.x - qr) / cell), (int)floorf((xi.y - qr) / cell), (int)floorf((xi.z - qr) / cell)};
+  int hi[3] = {(int)floorf((xi.x + qr) / cell), (int)floorf((xi.y + qr) / cell), (int)floorf((xi.z + qr) / cell)};
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = max(lo[d], b.red[d]);
+    hi[d] = min(hi[d], b.red[3 + d]);
+  }
+  for (int cx = lo[0]; cx <= hi[0]; ++cx)
+    for (int cy = lo[1]; cy <= hi[1]; ++cy)
+      for (int cz = lo[2]; cz <= hi[2]; ++cz) {
+        uint64_t key = cell_key(b.red, cx, cy, cz);
+        for (int q = lower_bound_key(b.ckey, s.n, key); q < s.n && b.ckey[q] == key; ++q) {
+          int j = (int)b.cval[q];
+          if (!keep_pair(s, i, j)) continue;
+          V3 e_j = v3(s.he[j]);
+          float rs_j = length(e_j);
+          float mj = fmin_r(dt * (length(v3(s.v[j])) + length(v3(s.w[j])) * rs_j), rs_j);
+          V3 half_j = aabb_half(q4(s.q[j]), e_j);
+          V3 dpos = xi - v3(s.x[j]);
+          float pad = man_margin + mi + mj;
+          float ox = fabsf(dpos.x) - (half_i.x + half_j.x + pad);
+          float oy = fabsf(dpos.y) - (half_i.y + half_j.y + pad);
+          float oz = fabsf(dpos.z) - (half_i.z + half_j.z + pad);
+          if (ox <= 0.0f && oy <= 0.0f && oz <= 0.0f) emit(j);
+        }
+      }
+}
+
+__global__ void k6_hg_count(Dev6 s, Par6 p, BP6 b, float rs_max, float cell) {
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    int cnt = 0;
+    hg_query(s, b, i, p.margin, p.dt, rs_max, cell, [&](int) { ++cnt; });
+    b.counts[i] = cnt;
+  }
+}
+
+__global__ void k6_hg_write(Dev6 s, Par6 p, BP6 b, float rs_max, float cell, int* status) {
+  const int total = *s.n_pairs;
+  if (gtid() == 0 && total > s.cap) raise_status(status, XPBD_ERR_OVERFLOW);
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    if (b.counts[i] == 0) continue;
+    const int base = b.offsets[i];
+    int r = 0;
+    hg_query(s, b, i, p.margin, p.dt, rs_max, cell, [&](int j) {
+      if (base + r < s.cap) s.pairs[base + r] = make_int2(i, j);
+      ++r;
+    });
+    sort_segment(s.pairs, base, min(base + r, s.cap));
+  }
+}
+
+// =================================================================================
+// Host-grid broad phase (solver_6dof.py:232-258 via _grid_candidate_pairs,
+// solver.py:514-562), on the device, in the reference's emission order.
+// =================================================================================
+__constant__ int kFwd6[14][3] = {{0, 0, 0},  {1, -1, -1}, {1, -1, 0}, {1, -1, 1}, {1, 0, -1},
+                                 {1, 0, 0},  {1, 0, 1},   {1, 1, -1}, {1, 1, 0},  {1, 1, 1},
+                                 {0, 1, -1}, {0, 1, 0},   {0, 1, 1},  {0, 0, 1}};
+
+// red[6] = max|v comp| bits, red[7] = max|w comp| bits, red[8] = max aabb half bits
+__global__ void k6_grid_reduce(Dev6 s, BP6 b) {
+  float vm = 0.0f, wm = 0.0f, hm = 0.0f;
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    float4 v = s.v[i], w = s.w[i];
+    vm = fmaxf(vm, fmaxf(fabsf(v.x), fmaxf(fabsf(v.y), fabsf(v.z))));
+    wm = fmaxf(wm, fmaxf(fabsf(w.x), fmaxf(fabsf(w.y), fabsf(w.z))));
+    V3 h = aabb_half(q4(s.q[i]), v3(s.he[i]));
+    b.half[i] = f4(h, 0.0f);
+    hm = fmaxf(hm, fmaxf(h.x, fmaxf(h.y, h.z)));
+  }
+  for (int o = 16; o; o >>= 1) {
+    vm = fmaxf(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+    wm = fmaxf(wm, __shfl_xor_sync(0xffffffffu, wm, o));
+    hm = fmaxf(hm, __shfl_xor_sync(0xffffffffu, hm, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&b.red[6], __float_as_int(vm));
+    atomicMax(&b.red[7], __float_as_int(wm));
+    atomicMax(&b.red[8], __float_as_int(hm));
+  }
+}
+
+XD void grid_margin(const BP6& b, double man_margin, double dt, double maxhe, float* cell_f, float* margin_f) {
+  double vmax = (double)__int_as_float(b.red[6]), wmax = (double)__int_as_float(b.red[7]);
+  double rmax = (double)__int_as_float(b.red[8]);
+  double margin = man_margin + 2.0 * dt * (vmax + wmax * maxhe);
+  if (rmax < margin) margin = rmax;
+  *cell_f = (float)(2.0 * rmax + margin);
+  *margin_f = (float)margin;
+}
+
+__global__ void k6_grid_cells(Dev6 s, BP6 b, double man_margin, double dt, double maxhe) {
+  float cell, marg;
+  grid_margin(b, man_margin, dt, maxhe, &cell, &marg);
+  int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (int i = gtid(); i < s.n; i += gstride()) {
+    float4 x = s.x[i];
+    int c[3] = {(int)floorf(x.x / cell), (int)floorf(x.y / cell), (int)floorf(x.z / cell)};
+    b.cell[i] = make_int4(c[0], c[1], c[2], 0);
+    for (int d = 0; d < 3; ++d) {
+      lmin[d] = min(lmin[d], c[d]);
+      lmax[d] = max(lmax[d], c[d]);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o; o >>= 1) {
+      lmin[d] = min(lmin[d], __shfl_xor_sync(0xffffffffu, lmin[d], o));
+      lmax[d] = max(lmax[d], __shfl_xor_sync(0xffffffffu, lmax[d], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&b.red[d], lmin[d]);
+      atomicMax(&b.red[3 + d], lmax[d]);
+    }
+  }
+}
+
+XD int64_t grid_S6(const int* red) {
+  int64_t ext = 0;
+  for (int d = 0; d < 3; ++d) ext = max(ext, (int64_t)red[3 + d] - (int64_t)red[d]);
+  return ext + 2;
+}
+
+__global__ void k6_grid_keys(int n, BP6 b) {
+  int64_t S = grid_S6(b.red);
+  for (int i = gtid(); i < n; i += gstride()) {
+    int4 c = b.cell[i];
+    int64_t id = (((int64_t)c.x - b.red[0]) * S + ((int64_t)c.y - b.red[1])) * S + ((int64_t)c.z - b.red[2]);
+    b.keys[i] = (uint64_t)id;   // unsorted copy (per body)
+    b.ckey[i] = (uint64_t)id;   // sorted below
+    b.cval[i] = (uint32_t)i;
+  }
+}
+
+template <class Emit>
+XD int grid_slot(const Dev6& s, const BP6& b, int o, int k, float margin_f, int64_t S, Emit emit) {
+  int64_t delta = ((int64_t)kFwd6[o][0] * S + kFwd6[o][1]) * S + kFwd6[o][2];
+  int64_t target = (int64_t)b.keys[k] + delta;
+  if (target < 0) return 0;
+  int cnt = 0;
+  float4 xa = s.x[k], ha = b.half[k];
+  for (int q = lower_bound_key(b.ckey, s.n, (uint64_t)target); q < s.n && b.ckey[q] == (uint64_t)target; ++q) {
+    int partner = (int)b.cval[q];
+    if (o == 0 && !(partner > k)) continue;
+    float4 xb = s.x[partner], hb = b.half[partner];
+    if (!(fabsf(xa.x - xb.x) - (ha.x + hb.x + margin_f) <= 0.0f)) continue;
+    if (!(fabsf(xa.y - xb.y) - (ha.y + hb.y + margin_f) <= 0.0f)) continue;
+    if (!(fabsf(xa.z - xb.z) - (ha.z + hb.z + margin_f) <= 0.0f)) continue;
+    if (!(xa.w > 0.0f || xb.w > 0.0f)) continue;
+    int ga = s.group[k];
+    if (ga == s.group[partner] && ga > 0) continue;
+    emit(cnt, partner);
+    ++cnt;
+  }
+  return cnt;
+}
+
+__global__ void k6_grid_count(Dev6 s, BP6 b, double man_margin, double dt, double maxhe) {
+  float cell, marg;
+  grid_margin(b, man_margin, dt, maxhe, &cell, &marg);
+  int64_t S = grid_S6(b.red);
+  for (int t = gtid(); t < 14 * s.n; t += gstride()) {
+    int o = t / s.n, k = t - o * s.n;
+    b.counts[t] = grid_slot(s, b, o, k, marg, S, [](int, int) {});
+  }
+}
+
+__global__ void k6_grid_write(Dev6 s, BP6 b, double man_margin, double dt, double maxhe, int* status) {
+  float cell, marg;
+  grid_margin(b, man_margin, dt, maxhe, &cell, &marg);
+  int64_t S = grid_S6(b.red);
+  const int total = *s.n_pairs;
+  if (gtid() == 0 && total > s.cap) raise_status(status, XPBD_ERR_OVERFLOW);
+  for (int t = gtid(); t < 14 * s.n; t += gstride()) {
+    if (b.counts[t] == 0) continue;
+    int o = t / s.n, k = t - o * s.n;
+    int base = b.offsets[t];
+    grid_slot(s, b, o, k, marg, S, [&](int r, int partner) {
+      if (base + r < s.cap) s.pairs[base + r] = make_int2(k, partner);
+    });
+  }
+}
+
+}  // namespace xpbd
+
+// =================================================================================
+// C ABI
+// =================================================================================
+using namespace xpbd;
+
+static Dev6 make_dev6(const xpbd6_state* s) {
+  Dev6 d;
+  d.x = reinterpret_cast<float4*>(s->x);
+  d.q = reinterpret_cast<float4*>(s->q);
+  d.v = reinterpret_cast<float4*>(s->v);
+  d.w = reinterpret_cast<float4*>(s->w);
+  d.xp = reinterpret_cast<float4*>(s->x_prev);
+  d.qp = reinterpret_cast<float4*>(s->q_prev);
+  d.inv_I = reinterpret_cast<const float4*>(s->inv_I);
+  d.he = reinterpret_cast<const float4*>(s->he);
+  d.group = s->group;
+  d.ax = reinterpret_cast<float4*>(s->acc_x);
+  d.ar = reinterpret_cast<float4*>(s->acc_r);
+  d.av = reinterpret_cast<float4*>(s->acc_v);
+  d.aw = reinterpret_cast<float4*>(s->acc_w);
+  d.lam_floor = s->lam_floor;
+  d.pairs = reinterpret_cast<int2*>(s->pairs);
+  d.n_pairs = s->n_pairs;
+  d.m_hdr = reinterpret_cast<int4*>(s->m_hdr);
+  d.m_normal = reinterpret_cast<float4*>(s->m_normal);
+  d.m_off_inc = reinterpret_cast<float4*>(s->m_off_inc);
+  d.m_off_ref = reinterpret_cast<float4*>(s->m_off_ref);
+  d.lam_pair = s->lam_pair;
+  d.j_ab = reinterpret_cast<const int2*>(s->j_ab);
+  d.j_a = reinterpret_cast<const float4*>(s->j_anchor_a);
+  d.j_b = reinterpret_cast<const float4*>(s->j_anchor_b);
+  d.lam_joint = s->lam_joint;
+  d.n = s->n_bodies;
+  d.nj = s->n_joints;
+  d.cap = s->pair_capacity;
+  return d;
+}
+
+static Par6 make_par6(const xpbd6_params* p) {
+  Par6 q;
+  q.h = (float)(p->dt / (double)(p->substeps > 0 ? p->substeps : 1));
+  q.dt = (float)p->dt;
+  q.gx = p->gravity[0];
+  q.gy = p->gravity[1];
+  q.gz = p->gravity[2];
+  q.floor_y = p->floor_y;
+  q.mu = p->friction;
+  q.rest = p->restitution;
+  q.lin_damp = p->lin_damp;
+  q.ang_damp = p->ang_damp;
+  q.relax = p->jacobi_relax;
+  q.max_speed = p->max_speed;
+  q.max_omega = p->max_omega;
+  q.margin = p->man_margin;
+  q.substeps = p->substeps;
+  q.iterations = p->iterations;
+  q.gyro = p->gyroscopic;
+  return q;
+}
+
+static int check6(const xpbd6_state* s) {
+  if (!s || s->n_bodies < 0 || s->n_joints < 0 || s->pair_capacity < 0 || !s->x || !s->q || !s->v || !s->w ||
+      !s->n_pairs)
+    return XPBD_ERR_BAD_ARG;
+  return XPBD_OK;
+}
+
+#define XPBD6_LAUNCH(kern, work, ...)                                                  \
+  do {                                                                                 \
+    if (check6(s) || !p) return XPBD_ERR_BAD_ARG;                                      \
+    long long w_ = (work);                                                             \
+    if (w_ <= 0) return XPBD_OK;                                                       \
+    kern<<<stream_blocks(w_, 256), 256, 0, as_stream(stream)>>>(__VA_ARGS__);          \
+    XPBD_LAUNCHED();                                                                   \
+    return XPBD_OK;                                                                    \
+  } while (0)
+
+extern "C" int xpbd6_integrate(const xpbd6_state* s, const xpbd6_params* p, void* stream) {
+  XPBD6_LAUNCH(k6_integrate, std::max(s->n_bodies, s->n_joints), make_dev6(s), make_par6(p));
+}
+extern "C" int xpbd6_manifold(const xpbd6_state* s, float margin, void* stream) {
+  const void* p = s;
+  XPBD6_LAUNCH(k6_manifold, s->pair_capacity, make_dev6(s), margin);
+}
+extern "C" int xpbd6_solve_positions(const xpbd6_state* s, const xpbd6_params* p, int first, void* stream) {
+  (void)first;
+  XPBD6_LAUNCH(k6_solve_positions, (long long)s->n_joints + s->n_bodies + s->pair_capacity, make_dev6(s),
+               make_par6(p));
+}
+extern "C" int xpbd6_apply_jacobi(const xpbd6_state* s, float relax, void* stream) {
+  const void* p = s;
+  XPBD6_LAUNCH(k6_apply, s->n_bodies, make_dev6(s), relax);
+}
+extern "C" int xpbd6_finalize(const xpbd6_state* s, const xpbd6_params* p, void* stream) {
+  XPBD6_LAUNCH(k6_finalize, s->n_bodies, make_dev6(s), make_par6(p));
+}
+extern "C" int xpbd6_solve_velocities(const xpbd6_state* s, const xpbd6_params* p, void* stream) {
+  XPBD6_LAUNCH(k6_solve_velocities, (long long)s->n_bodies + s->pair_capacity, make_dev6(s), make_par6(p));
+}
+extern "C" int xpbd6_apply_velocity(const xpbd6_state* s, const xpbd6_params* p, void* stream) {
+  XPBD6_LAUNCH(k6_apply_velocity, s->n_bodies, make_dev6(s), make_par6(p));
+}
+
+__global__ void k6_body_aabb(Dev6 s, Par6 p, float4* lo, float4* hi) {
+  for (int i = gtid(); i < s.n; i += gstride()) body_aabb(s, i, p.margin, p.dt, lo, hi);
+}
+extern "C" int xpbd6_body_aabb(const xpbd6_state* s, const xpbd6_params* p, float* lowers, float* uppers,
+                               void* stream) {
+  if (!lowers || !uppers) return XPBD_ERR_BAD_ARG;
+  XPBD6_LAUNCH(k6_body_aabb, s->n_bodies, make_dev6(s), make_par6(p), reinterpret_cast<float4*>(lowers),
+               reinterpret_cast<float4*>(uppers));
+}
+
+// ---- solver handle ------------------------------------------------------------------
+struct xpbd6_solver {
+  xpbd6_state st{};
+  xpbd6_params par{};
+  Dev6 dev{};
+  Par6 p6{};
+  BP6 bp{};
+  void* buf = nullptr;
+  size_t buf_bytes = 0;
+  unsigned* bar = nullptr;  // count, gen, status
+  int blocks = 1, threads = 256;
+  int force_blocks = 0;
+  double hg_rsmax = 0.0, hg_cell = 0.0, maxhe = 0.0;
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;
+};
+
+static void free_graph(xpbd6_solver* h) {
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+}
+
+extern "C" int xpbd6_create(xpbd6_solver** out) {
+  if (!out) return XPBD_ERR_BAD_ARG;
+  xpbd6_solver* h = new xpbd6_solver();
+  cudaError_t e = cudaMalloc(&h->bar, 4 * sizeof(unsigned));
+  if (e != cudaSuccess) {
+    set_last_error("cudaMalloc", e);
+    delete h;
+    return XPBD_ERR_CUDA;
+  }
+  cudaMemset(h->bar, 0, 4 * sizeof(unsigned));
+  *out = h;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd6_destroy(xpbd6_solver* h) {
+  if (!h) return XPBD_OK;
+  free_graph(h);
+  if (h->buf) cudaFree(h->buf);
+  if (h->bar) cudaFree(h->bar);
+  delete h;
+  return XPBD_OK;
+}
+
+// Testing hook: fixed number of blocks for the persistent substep kernel (0 = auto).
+extern "C" int xpbd6_force_blocks(xpbd6_solver* h, int blocks) {
+  if (!h || blocks < 0) return XPBD_ERR_BAD_ARG;
+  h->force_blocks = blocks;
+  return XPBD_OK;
+}
+
+// Host constants of the hash-grid and grid broad phases (solver_6dof.py:335-337, 244).
+extern "C" int xpbd6_set_grid_constants(xpbd6_solver* h, double rs_max, double cell, double max_he) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  h->hg_rsmax = rs_max;
+  h->hg_cell = cell;
+  h->maxhe = max_he;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_params* p) {
+  if (!h || check6(s) || !p) return XPBD_ERR_BAD_ARG;
+  if (p->substeps < 0 || p->iterations < 0 || p->broadphase < 0 || p->broadphase > 2) return XPBD_ERR_BAD_ARG;
+  free_graph(h);
+  h->st = *s;
+  h->par = *p;
+  h->dev = make_dev6(s);
+  h->p6 = make_par6(p);
+  const int n = std::max(s->n_bodies, 2);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  size_t o_lo = take(16 * (size_t)n), o_hi = take(16 * (size_t)n), o_b = take(64), o_k = take(8 * (size_t)n),
+         o_v = take(4 * (size_t)n), o_st = take(sort_scratch_bytes(n)), o_ch = take(8 * (size_t)n),
+         o_par = take(4 * 2 * (size_t)n), o_nlo = take(16 * 2 * (size_t)n), o_nhi = take(16 * 2 * (size_t)n),
+         o_fl = take(4 * (size_t)n), o_cnt = take(4 * 14 * (size_t)n), o_off = take(4 * 14 * (size_t)n),
+         o_sc = take(scan_scratch_bytes(14 * n)), o_cell = take(16 * (size_t)n), o_ck = take(8 * (size_t)n),
+         o_cv = take(4 * (size_t)n), o_red = take(64), o_half = take(16 * (size_t)n);
+  if (off > h->buf_bytes) {
+    if (h->buf) cudaFree(h->buf);
+    h->buf = nullptr;
+    XPBD_CUDA(cudaMalloc(&h->buf, off));
+    h->buf_bytes = off;
+  }
+  char* b = static_cast<char*>(h->buf);
+  BP6& q = h->bp;
+  q.lo = reinterpret_cast<float4*>(b + o_lo);
+  q.hi = reinterpret_cast<float4*>(b + o_hi);
+  q.bounds = reinterpret_cast<int*>(b + o_b);
+  q.keys = reinterpret_cast<uint64_t*>(b + o_k);
+  q.vals = reinterpret_cast<uint32_t*>(b + o_v);
+  q.sort_tmp = b + o_st;
+  q.child = reinterpret_cast<int2*>(b + o_ch);
+  q.parent = reinterpret_cast<int*>(b + o_par);
+  q.nlo = reinterpret_cast<float4*>(b + o_nlo);
+  q.nhi = reinterpret_cast<float4*>(b + o_nhi);
+  q.flags = reinterpret_cast<int*>(b + o_fl);
+  q.counts = reinterpret_cast<int*>(b + o_cnt);
+  q.offsets = reinterpret_cast<int*>(b + o_off);
+  q.scan_tmp = b + o_sc;
+  q.cell = reinterpret_cast<int4*>(b + o_cell);
+  q.ckey = reinterpret_cast<uint64_t*>(b + o_ck);
+  q.cval = reinterpret_cast<uint32_t*>(b + o_cv);
+  q.red = reinterpret_cast<int*>(b + o_red);
+  q.half = reinterpret_cast<float4*>(b + o_half);
+  int per_sm = 0;
+  XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k6_substeps, 256, 0));
+  per_sm = std::max(per_sm, 1);
+  long long work = std::max<long long>((long long)s->n_bodies + s->n_joints, s->pair_capacity / 2);
+  int want = std::max(1, ceil_div(work, 256));
+  h->blocks = std::min(want, per_sm * num_sms());
+  if (h->force_blocks > 0) h->blocks = std::min(h->force_blocks, per_sm * num_sms());
+  h->threads = 256;
+  return XPBD_OK;
+}
+
+static int run_broadphase(xpbd6_solver* h, cudaStream_t st) {
+  const Dev6& s = h->dev;
+  const BP6& b = h->bp;
+  const int n = s.n;
+  int* status = reinterpret_cast<int*>(h->bar + 2);
+  if (n < 2) {
+    XPBD_CUDA(cudaMemsetAsync(s.n_pairs, 0, sizeof(int), st));
+    return XPBD_OK;
+  }
+  const int blocks = stream_blocks(n, 256);
+  int rc;
+  if (h->par.broadphase == 0) {
+    k6_bp_init<<<1, 32, 0, st>>>(b);
+    k6_aabb<<<blocks, 256, 0, st>>>(s, h->p6, b);
+    k6_morton<<<blocks, 256, 0, st>>>(n, b);
+    XPBD_LAUNCHED();
+    if ((rc = sort_pairs_u64(b.keys, b.vals, n, b.sort_tmp, 30, st))) return rc;
+    k6_build<<<stream_blocks(n - 1, 256), 256, 0, st>>>(n, b);
+    k6_refit<<<blocks, 256, 0, st>>>(n, b);
+    k6_pairs_count<<<blocks, 256, 0, st>>>(s, b, status);
+    XPBD_LAUNCHED();
+    if ((rc = exclusive_scan_i32(b.counts, b.offsets, n, s.n_pairs, b.scan_tmp, st))) return rc;
+    k6_pairs_write<<<blocks, 256, 0, st>>>(s, b, status);
+  } else if (h->par.broadphase == 1) {
+    float cell = (float)h->hg_cell, rsmax = (float)h->hg_rsmax;
+    k6_red_init<<<1, 32, 0, st>>>(b);
+    k6_hg_cells<<<blocks, 256, 0, st>>>(s, h->p6, b, cell);
+    k6_hg_keys<<<blocks, 256, 0, st>>>(n, b);
+    XPBD_LAUNCHED();
+    if ((rc = sort_pairs_u64(b.ckey, b.cval, n, b.sort_tmp, 63, st))) return rc;
+    k6_hg_count<<<blocks, 256, 0, st>>>(s, h->p6, b, rsmax, cell);
+    XPBD_LAUNCHED();
+    if ((rc = exclusive_scan_i32(b.counts, b.offsets, n, s.n_pairs, b.scan_tmp, st))) return rc;
+    k6_hg_write<<<blocks, 256, 0, st>>>(s, h->p6, b, rsmax, cell, status);
+  } else {
+    double mm = (double)h->par.man_margin, dt = h->par.dt;
+    k6_red_init<<<1, 32, 0, st>>>(b);
+    k6_grid_reduce<<<blocks, 256, 0, st>>>(s, b);
+    k6_grid_cells<<<blocks, 256, 0, st>>>(s, b, mm, dt, h->maxhe);
+    k6_grid_keys<<<blocks, 256, 0, st>>>(n, b);
+    XPBD_LAUNCHED();
+    if ((rc = sort_pairs_u64(b.ckey, b.cval, n, b.sort_tmp, 63, st))) return rc;
+    const int bt = stream_blocks(14LL * n, 128);
+    k6_grid_count<<<bt, 128, 0, st>>>(s, b, mm, dt, h->maxhe);
+    XPBD_LAUNCHED();
+    if ((rc = exclusive_scan_i32(b.counts, b.offsets, 14 * n, s.n_pairs, b.scan_tmp, st))) return rc;
+    k6_grid_write<<<bt, 128, 0, st>>>(s, b, mm, dt, h->maxhe, status);
+  }
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+static int run_substeps(xpbd6_solver* h, cudaStream_t st) {
+  if (h->dev.n == 0) return XPBD_OK;
+  GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2)};
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(h->blocks);
+  cfg.blockDim = dim3(h->threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = h->blocks > 1 ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  XPBD_CUDA(cudaLaunchKernelEx(&cfg, k6_substeps, h->dev, h->p6, gb));
+  return XPBD_OK;
+}
+
+extern "C" int xpbd6_broadphase(xpbd6_solver* h, void* stream) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  return run_broadphase(h, as_stream(stream));
+}
+
+extern "C" int xpbd6_substeps(xpbd6_solver* h, void* stream) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  return run_substeps(h, as_stream(stream));
+}
+
+// One frame = broad phase + substeps, captured once as a CUDA graph and replayed.
+extern "C" int xpbd6_step(xpbd6_solver* h, int frames, void* stream) {
+  if (!h || frames < 0) return XPBD_ERR_BAD_ARG;
+  if (frames == 0 || h->dev.n == 0) return XPBD_OK;
+  cudaStream_t st = as_stream(stream);
+  if (!h->graph) {
+    cudaStream_t cap;
+    XPBD_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    XPBD_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    int rc = run_broadphase(h, cap);
+    if (!rc) rc = run_substeps(h, cap);
+    cudaError_t e = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (rc) return rc;
+    XPBD_CUDA(e);
+    e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    XPBD_CUDA(e);
+  }
+  for (int f = 0; f < frames; ++f) XPBD_CUDA(cudaGraphLaunch(h->graph, st));
+  return XPBD_OK;
+}
+
+extern "C" int xpbd6_status(xpbd6_solver* h, int* out, void* stream) {
+  if (!h || !out) return XPBD_ERR_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  XPBD_CUDA(cudaMemcpyAsync(out, h->bar + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+  XPBD_CUDA(cudaStreamSynchronize(st));
+  XPBD_CUDA(cudaMemsetAsync(h->bar + 2, 0, sizeof(int), st));
+  return XPBD_OK;
+}
+
+extern "C" int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream) {
+  if (!h || !codes_out) return XPBD_ERR_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  const int n = h->dev.n;
+  if (n == 0) return XPBD_OK;
+  k6_bp_init<<<1, 32, 0, st>>>(h->bp);
+  k6_aabb<<<stream_blocks(n, 256), 256, 0, st>>>(h->dev, h->p6, h->bp);
+  k6_morton<<<stream_blocks(n, 256), 256, 0, st>>>(n, h->bp);
+  XPBD_LAUNCHED();
+  std::vector<uint64_t> k(n);
+  XPBD_CUDA(cudaMemcpyAsync(k.data(), h->bp.keys, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  XPBD_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < n; ++i) codes_out[i] = (unsigned)k[i];
+  return XPBD_OK;
+}
+
+extern "C" int xpbd6_launch_info(xpbd6_solver* h, int* blocks, int* threads) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  if (blocks) *blocks = h->blocks;
+  if (threads) *threads = h->threads;
+  return XPBD_OK;
+}
