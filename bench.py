@@ -267,84 +267,53 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
 
 
 def time_e2e(args, workload, device):
-    if workload in SIX_DOF:
-        return time_e2e6(args, workload, device)
-    """Same metric through the public API with host buffers: each frame uploads
-    the particle state from pinned host memory, steps, and reads the positions
-    back into pinned host memory, all inside the CUDA-event-timed region."""
+    """Same metric through the public API with host buffers.  Every frame: the
+    state (3-DOF: x, v; 6-DOF: x, q, v, w) is uploaded from pinned host memory,
+    ``step()`` runs, and the state is read back into pinned host memory, which
+    feeds the next frame; the stream is synchronised each frame.  The region is
+    bracketed by CUDA events on the solver's stream."""
     import torch
 
-    from xpbd_b200 import Solver
-    s = make_solver(workload, device, Solver)
-    s.sync_contacts = False
+    from xpbd_b200 import Solver, Solver6DOF
+    six = workload in SIX_DOF
+    s = make_solver(workload, device, Solver6DOF if six else Solver)
+    if six:
+        s.sync_pairs = False
+    else:
+        s.sync_contacts = False
     s._flush()
     T = s.tensors
-    hx = T["x"].cpu().pin_memory()
-    hv = T["v"].cpu().pin_memory()
-    out = torch.empty_like(hx).pin_memory()
-    stream = torch.cuda.current_stream(device)
-    for _ in range(max(3, args.warmup // 2)):
-        T["x"].copy_(hx, non_blocking=True); T["v"].copy_(hv, non_blocking=True)
-        s.step()
-        out.copy_(T["x"], non_blocking=True)
-        hx.copy_(out)
-    torch.cuda.synchronize(device)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    steps = max(1, args.steps // 2)
-    e0.record(stream)
-    for _ in range(steps):
-        T["x"].copy_(hx, non_blocking=True)
-        T["v"].copy_(hv, non_blocking=True)
-        s.step()
-        out.copy_(T["x"], non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize(device)
-    ms = e0.elapsed_time(e1) / steps
-    m = s.num_constraints
-    h2d = hx.numel() * 4 + hv.numel() * 4
-    d2h = out.numel() * 4
-    return ms, m * s.substeps * s.iterations, h2d, d2h
-
-
-def time_e2e6(args, workload, device):
-    """6-DOF end to end: upload positions/orientations/velocities from pinned
-    host memory, step through the public API (graph replay), read back
-    positions and orientations, inside the timed region."""
-    import torch
-
-    from xpbd_b200 import Solver6DOF
-    s = make_solver(workload, device, Solver6DOF)
-    s.sync_pairs = False
-    s._flush()
-    T = s.tensors
-    keys = ("x", "q", "v", "w")
+    keys = ("x", "q", "v", "w") if six else ("x", "v")
     host = {k: T[k].cpu().pin_memory() for k in keys}
-    outx = torch.empty_like(host["x"]).pin_memory()
-    outq = torch.empty_like(host["q"]).pin_memory()
     stream = torch.cuda.current_stream(device)
-    steps = max(1, args.steps // 2)
-    for _ in range(3):
-        s.step()
-    torch.cuda.synchronize(device)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
+
+    def frame():
         for k in keys:
             T[k].copy_(host[k], non_blocking=True)
         s.step()
-        outx.copy_(T["x"], non_blocking=True)
-        outq.copy_(T["q"], non_blocking=True)
+        for k in keys:
+            host[k].copy_(T[k], non_blocking=True)
+        stream.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        frame()
+    steps = max(1, args.steps // 2)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        frame()
     e1.record(stream)
     torch.cuda.synchronize(device)
     ms = e0.elapsed_time(e1) / steps
-    n_dyn = int((T["x"][:, 3] > 0).sum().item())
-    hdr = T["m_hdr"][:min(s.n_pairs, s.cap)].cpu().numpy()
-    proj = (8 * n_dyn + int(hdr[:, 0].sum()) + s.num_joints) * s.substeps * s.iterations
-    h2d = sum(host[k].numel() * 4 for k in keys)
-    d2h = (outx.numel() + outq.numel()) * 4
-    return ms, proj, h2d, d2h
+    if six:
+        n_dyn = int((T["x"][:, 3] > 0).sum().item())
+        hdr = T["m_hdr"][:min(s.n_pairs, s.cap)].cpu().numpy()
+        rows = 8 * n_dyn + int(hdr[:, 0].sum()) + s.num_joints
+    else:
+        rows = s.num_constraints
+    nbytes = sum(host[k].numel() * 4 for k in keys)
+    return ms, rows * s.substeps * s.iterations, nbytes, nbytes
 
 
 def cpu_baseline(workload, seconds):
@@ -428,6 +397,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only the device-timed loop (for profiler launch lists): no e2e, CPU baseline or extras")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -477,6 +448,9 @@ def main():
             "status_bits": r["status"],
         }
         line["clocks"] = clocks.summary()
+        if args.kernels_only:
+            print(json.dumps(line), flush=True)
+            return
         try:
             e_ms, e_proj, h2d, d2h = time_e2e(args, args.workload, device)
             line["e2e"] = {"value": round(world * e_proj / (e_ms / 1e3) / 1e6, 4), "unit": "M proj/s",
