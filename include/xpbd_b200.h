@@ -128,6 +128,22 @@ int xpbd3_contacts_build(xpbd3_contacts* c, const xpbd3_state* s, const float* r
                          double contact_margin, double dt, double r_max, int* status_dev,
                          void* stream);
 
+/* No counterpart in the reference.  Same contact rows as xpbd3_contacts_build,
+ * for callers that cannot allocate device memory while they step (a plugin
+ * whose host owns all GPU allocations, or a fixed-budget simulation thread for
+ * which cudaMalloc's device-wide synchronisation is off limits): all working
+ * memory comes from one fixed device array inside the library (about 1.4 MB,
+ * held on every GPU that loads the library until exit) and the call performs
+ * no allocation.  At most 8192 collidable spheres; larger n_collide returns
+ * XPBD_ERR_BAD_ARG.  The first call on a device looks the array's address up
+ * (make it before any stream capture).  All calls on a device share the array:
+ * calls on one stream run back to back safely, calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+int xpbd3_contacts_build_noalloc(const xpbd3_state* s, const float* radius, const float* friction,
+                                 const int* collide_idx, int n_collide, const int64_t* existing,
+                                 int n_existing, const float* x_init, double contact_margin, double dt,
+                                 double r_max, int* status_dev, void* stream);
+
 /* Device primitives exposed for tests (no reference counterpart): stable sort
  * of uint64 keys with uint32 values, and exclusive scan of int32. */
 int xpbd_sort_pairs_u64(uint64_t* keys, uint32_t* vals, int n, int max_bits, void* stream);

@@ -16,6 +16,7 @@
 //   5. counts per (o, k) are scanned, and the pairs are written at their scan
 //      offsets -- offset-major, then k, then partner: the reference's order.
 #include <algorithm>
+#include <mutex>
 
 #include "prims.cuh"
 
@@ -337,6 +338,148 @@ extern "C" int xpbd3_contacts_build(xpbd3_contacts* c, const xpbd3_state* st, co
   rc = exclusive_scan_i32(c->s.counts, c->s.offsets, 14 * a.m, c->s.total, c->s.scan_tmp, s);
   if (rc) return rc;
   kc_write<<<blocks_t, 128, 0, s>>>(a, c->s);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+// =============================================================================
+// Allocation-free variant of xpbd3_contacts_build.
+//
+// Some hosts cannot allocate device memory at the point where they step the
+// scene: a plugin whose host application owns every GPU allocation through its
+// own allocator, or a fixed-budget simulation thread for which cudaMalloc is
+// off limits because it can synchronise the whole device and stall for
+// milliseconds.  This entry point generates the same contact rows as
+// xpbd3_contacts_build but takes its working memory from a fixed, file-scope
+// device array instead of a handle's cudaMalloc'd buffer.
+//
+// Limits and rules:
+//  * at most kNoAllocMaxCollide collidable spheres (8192); larger inputs are
+//    rejected with XPBD_ERR_BAD_ARG before anything is launched;
+//  * the array (about 1.4 MB) lives on every GPU that loads the library until
+//    the process exits;
+//  * the first call on a device looks the array's device address up with
+//    cudaGetSymbolAddress (with that device current) and caches it per device;
+//    make that first call before any stream capture begins;
+//  * every call on a device shares the one array and each call re-initialises
+//    what it needs (reductions, counts, offsets and totals are rewritten before
+//    they are read), so back-to-back calls on one stream are fine but calls
+//    that overlap on the GPU (different streams, or concurrent host threads)
+//    race on the array and must be serialised by the caller;
+//  * it calls no cudaMalloc, cudaFree or allocating library routine.
+// =============================================================================
+namespace xpbd {
+
+constexpr int kNoAllocMaxCollide = 8192;
+
+constexpr size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+struct NoAllocLayout {
+  static constexpr size_t m = kNoAllocMaxCollide;
+  static constexpr size_t red = 0;
+  static constexpr size_t cell = red + align256(sizeof(ContactRed));
+  static constexpr size_t cid = cell + align256(sizeof(int4) * m);
+  static constexpr size_t skey = cid + align256(8 * m);
+  static constexpr size_t sval = skey + align256(8 * m);
+  static constexpr size_t counts = sval + align256(4 * m);
+  static constexpr size_t offsets = counts + align256(4 * 14 * m);
+  static constexpr size_t total = offsets + align256(4 * 14 * m);
+  static constexpr size_t sort_tmp = total + align256(16);
+  static constexpr size_t sort_bytes = m * (sizeof(uint64_t) + sizeof(uint32_t)) + 16;
+  static constexpr size_t scan_tmp = sort_tmp + align256(sort_bytes);
+  // one int per 4096-element scan tile of 14 m counts, plus slack
+  static constexpr size_t scan_bytes = ((14 * m + 4095) / 4096) * sizeof(int) + 16;
+  static constexpr size_t bytes = scan_tmp + align256(scan_bytes);
+};
+
+static __device__ __align__(256) unsigned char g_contacts_scratch[NoAllocLayout::bytes];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of g_contacts_scratch on the current device (looked up once).
+static int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  XPBD_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return XPBD_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    XPBD_CUDA(cudaGetSymbolAddress(&p, g_contacts_scratch));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  return XPBD_OK;
+}
+
+}  // namespace xpbd
+
+extern "C" int xpbd3_contacts_build_noalloc(const xpbd3_state* st, const float* radius, const float* friction,
+                                            const int* collide_idx, int n_collide, const int64_t* existing,
+                                            int n_existing, const float* x_init, double contact_margin,
+                                            double dt, double r_max, int* status_dev, void* stream) {
+  if (!st || n_collide < 0 || n_collide > kNoAllocMaxCollide || !x_init || !radius || !friction ||
+      (n_collide > 0 && !collide_idx) || (n_existing > 0 && !existing) || !st->n_rows)
+    return XPBD_ERR_BAD_ARG;
+  // sort_scratch_bytes / scan_scratch_bytes of the largest accepted input must fit the layout
+  if (sort_scratch_bytes(kNoAllocMaxCollide) > NoAllocLayout::sort_bytes ||
+      scan_scratch_bytes(14 * kNoAllocMaxCollide) > NoAllocLayout::scan_bytes)
+    return XPBD_ERR_BAD_ARG;
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  ContactScratch sc;
+  sc.red = reinterpret_cast<ContactRed*>(base + NoAllocLayout::red);
+  sc.cell = reinterpret_cast<int4*>(base + NoAllocLayout::cell);
+  sc.cid = reinterpret_cast<int64_t*>(base + NoAllocLayout::cid);
+  sc.skey = reinterpret_cast<uint64_t*>(base + NoAllocLayout::skey);
+  sc.sval = reinterpret_cast<uint32_t*>(base + NoAllocLayout::sval);
+  sc.counts = reinterpret_cast<int*>(base + NoAllocLayout::counts);
+  sc.offsets = reinterpret_cast<int*>(base + NoAllocLayout::offsets);
+  sc.total = reinterpret_cast<int*>(base + NoAllocLayout::total);
+  sc.sort_tmp = base + NoAllocLayout::sort_tmp;
+  sc.scan_tmp = base + NoAllocLayout::scan_tmp;
+  cudaStream_t s = as_stream(stream);
+  ContactArgs a{};
+  a.x = reinterpret_cast<float4*>(st->x);
+  a.v = reinterpret_cast<float4*>(st->v);
+  a.x_init = reinterpret_cast<const float4*>(x_init);
+  a.radius = radius;
+  a.friction = friction;
+  a.coll = collide_idx;
+  a.existing = existing;
+  a.n_existing = n_existing;
+  a.n = st->n_bodies;
+  a.m = n_collide;
+  a.contact_margin = contact_margin;
+  a.dt = dt;
+  a.rmax = r_max;
+  a.ri = reinterpret_cast<int4*>(st->row_i);
+  a.rf = reinterpret_cast<float4*>(st->row_f);
+  a.ra = reinterpret_cast<float4*>(st->row_anchor);
+  a.n_rows = st->n_rows;
+  a.n_static = st->n_rows_static;
+  a.cap_contacts = st->row_capacity - st->n_rows_static;
+  a.status = status_dev;
+  if (a.n == 0) return XPBD_OK;
+  kc_init<<<1, 32, 0, s>>>(sc.red);
+  kc_sanitize<<<stream_blocks(a.n, 256), 256, 0, s>>>(a, sc.red);
+  if (a.m < 2) {
+    kc_no_contacts<<<1, 32, 0, s>>>(a);
+    XPBD_LAUNCHED();
+    return XPBD_OK;
+  }
+  int blocks_m = stream_blocks(a.m, 256);
+  kc_cells<<<blocks_m, 256, 0, s>>>(a, sc);
+  kc_keys<<<blocks_m, 256, 0, s>>>(a, sc);
+  XPBD_LAUNCHED();
+  rc = sort_pairs_u64(sc.skey, sc.sval, a.m, sc.sort_tmp, 63, s);
+  if (rc) return rc;
+  int blocks_t = stream_blocks(14LL * a.m, 128);
+  kc_count<<<blocks_t, 128, 0, s>>>(a, sc);
+  rc = exclusive_scan_i32(sc.counts, sc.offsets, 14 * a.m, sc.total, sc.scan_tmp, s);
+  if (rc) return rc;
+  kc_write<<<blocks_t, 128, 0, s>>>(a, sc);
   XPBD_LAUNCHED();
   return XPBD_OK;
 }
