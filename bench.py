@@ -166,6 +166,7 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
         N.check(L.xpbd3_step(s._h, 1, sp), "xpbd3_step")
 
     s._flush()
+    tune = s.autotune(frames=3)
     for _ in range(args.warmup):
         frame()
     torch.cuda.synchronize(device)
@@ -203,7 +204,7 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
                launches=launches_per_frame * args.steps, solver=s)
     blocks, threads, smem = C.c_int(), C.c_int(), C.c_int()
     L.xpbd3_launch_info(s._h, C.byref(blocks), C.byref(threads), C.byref(smem))
-    res["launch"] = dict(blocks=blocks.value, threads=threads.value, smem_bytes=smem.value)
+    res["launch"] = dict(s.launch_info(), autotune=tune["ms_per_frame"])
     return res
 
 
@@ -223,6 +224,9 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
     L = lib6()
     stream = torch.cuda.current_stream(device)
     sp = N.stream_of(device)
+    for _ in range(3):   # let the pile develop contacts before tuning
+        N.check(L.xpbd6_step(s._h, 1, sp))
+    tune = s.autotune(frames=3)
     for _ in range(args.warmup):
         N.check(L.xpbd6_step(s._h, 1, sp))
     torch.cuda.synchronize(device)
@@ -263,7 +267,8 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
     alg = S * (I * (points * 196 + 8 * n_dyn * 47 + s.num_joints * 196) + npairs * 300 + n * 128)
     return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=kern_ms, proj_per_frame=proj_per_frame,
                 rows=rows, bodies=n, status=status, alg_bytes=alg, launches=args.steps * 16, solver=s,
-                launch={"pairs": npairs, "manifold_points": points, "graph_ms_per_frame": round(graph_ms, 5)})
+                launch=dict(s.launch_info(), pairs=npairs, manifold_points=points,
+                            graph_ms_per_frame=round(graph_ms, 5), autotune=tune["ms_per_frame"]))
 
 
 def time_e2e(args, workload, device):

@@ -101,8 +101,14 @@ int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_params* p);
 int xpbd3_step(xpbd3_solver* h, int frames, void* stream);
 /* Copies the device status word (XPBD_ERR_* bits) to *out and clears it. */
 int xpbd3_status(xpbd3_solver* h, int* out, void* stream);
-/* Launch configuration chosen by the last bind: blocks, threads, shared bytes. */
+/* Launch configuration chosen by the last bind: blocks (negative = that many
+ * CTAs forming one thread-block cluster), threads, shared bytes. */
 int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int* smem_bytes);
+/* Frame driver for the next bind (no reference counterpart; the autotuner's
+ * hook): mode -1 automatic, 0 cooperative grid with a bounded global barrier,
+ * 1 one CTA with the particle state in shared memory, 2 one thread-block
+ * cluster (2-16 CTAs, hardware cluster barrier); blocks/threads 0 = automatic. */
+int xpbd3_set_driver(xpbd3_solver* h, int mode, int blocks, int threads);
 
 /* coloring.py:26-71 color_constraints (host, Welsh-Powell, bit-exact order).
  * Returns the number of colors, or -1 on bad arguments. */
@@ -222,6 +228,14 @@ int xpbd6_substeps(xpbd6_solver* h, void* stream);
 /* broad phase + substeps, captured as one CUDA graph per frame. */
 int xpbd6_step(xpbd6_solver* h, int frames, void* stream);
 int xpbd6_status(xpbd6_solver* h, int* out, void* stream);
+/* Substep driver for the next bind (no reference counterpart): mode -1
+ * automatic, 0 cooperative grid, 2 one thread-block cluster. */
+int xpbd6_set_driver(xpbd6_solver* h, int mode, int blocks, int threads);
+/* blocks (negative = cluster of that many CTAs) and threads of the substep kernel. */
+int xpbd6_launch_info(xpbd6_solver* h, int* blocks, int* threads);
+/* Host constants of the hash-grid / grid broad phases (solver_6dof.py:335-337,
+ * 244): largest bounding radius |he|, hash-grid cell, largest |he| for the grid margin. */
+int xpbd6_set_grid_constants(xpbd6_solver* h, double rs_max, double cell, double max_he);
 /* Morton keys of the LBVH over lowers/uppers (float4[n]) -> uint32[n]. */
 int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream);
 

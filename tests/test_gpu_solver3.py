@@ -70,25 +70,39 @@ def test_one_substep_cloth32(mode):
 
 
 @pytest.mark.parametrize("mode", ["gs", "jacobi"])
-def test_shared_and_global_drivers_agree(mode):
-    """The single-CTA shared-memory driver and the cooperative grid driver run
-    the same phases; GS must agree exactly, Jacobi to atomic-order rounding."""
+def test_frame_drivers_agree(mode):
+    """Shared-memory single CTA, thread-block cluster and cooperative grid run
+    the same phases: GS must agree exactly, Jacobi to atomic-order rounding."""
     build = lambda s: scenes.build_cloth(s, res=12, spacing=0.05, y=0.01, velocity=(0.2, -1.0, 0.1))  # noqa: E731
-    res = []
-    for force in (1, 0):
+    res = {}
+    for drv, want in (((1, 0, 0), "shared"), ((2, 16, 1024), "cluster"), ((2, 4, 256), "cluster"),
+                      ((0, 0, 256), "grid"), ((0, 1, 256), "grid")):
         s = Solver(device="cuda:0", dt=1 / 60, substeps=15, iterations=2, solve_mode=mode)
         build(s)
-        s._flush()
-        N.check(N.lib().xpbd3_force_mode(s._h, force))
-        s._bind()
-        blocks, threads, smem = C.c_int(), C.c_int(), C.c_int()
-        N.lib().xpbd3_launch_info(s._h, C.byref(blocks), C.byref(threads), C.byref(smem))
-        assert (smem.value > 0) == (force == 1)
+        s.set_driver(*drv)
+        info = s.launch_info()
+        assert info["mode"] == want, info
         for _ in range(3):
             s.step()
-        res.append(s.positions())
-    d = np.abs(res[0] - res[1]).max()
-    assert d <= (0.0 if mode == "gs" else 1e-4), d
+        res[drv] = s.positions()
+        assert s.status() == 0
+    ref = res[(1, 0, 0)]
+    for drv, x in res.items():
+        d = np.abs(x - ref).max()
+        assert d <= (0.0 if mode == "gs" else 1e-4), (drv, d)
+
+
+def test_autotune_keeps_results():
+    o = O.OracleSolver(device="cpu", dt=1 / 60, substeps=15, iterations=2, solve_mode="gs")
+    s = Solver(device="cuda:0", dt=1 / 60, substeps=15, iterations=2, solve_mode="gs")
+    for t in (s, o):
+        scenes.build_cloth(t, res=16, spacing=0.03, y=0.01, velocity=(0.1, -0.5, 0.0))
+    rep = s.autotune(frames=2)
+    assert rep["chosen"]["mode"] in ("shared", "cluster", "grid")
+    for _ in range(2):
+        s.step()
+        o.step()
+    assert np.abs(s.positions() - o.positions()).max() <= 1e-6
 
 
 def test_multi_frame_launch_equals_single_frames():

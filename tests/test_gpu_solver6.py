@@ -92,16 +92,31 @@ def test_graph_frame_equals_synced_frame():
     assert np.abs(a - b).max() <= 1e-4
 
 
-def test_single_block_and_grid_drivers_agree():
-    res = []
-    for fb in (1, 0):
+def test_substep_drivers_agree():
+    res = {}
+    for drv, want in (((2, 16, 512), "cluster"), ((2, 4, 256), "cluster"), ((0, 0, 256), "grid"),
+                      ((0, 1, 256), "grid")):
         s = Solver6DOF(device="cuda:0", substeps=10, iterations=2, restitution=0.2)
-        s.force_blocks = fb
+        s.set_driver(*drv)
         scenes.build_box_pile(s, nx=4, ny=3, nz=4, pitch=0.55, seed=5)
+        assert s.launch_info()["mode"] == want
         for _ in range(3):
             s.step()
-        res.append(s.positions())
-    assert np.abs(res[0] - res[1]).max() <= 1e-4
+        assert s.status() == 0
+        res[drv] = s.positions()
+    ref = res[(2, 16, 512)]
+    for drv, x in res.items():
+        assert np.abs(x - ref).max() <= 1e-4, drv
+
+
+def test_autotune6_matches_oracle():
+    kw = dict(substeps=10, iterations=2, restitution=0.2)
+    eng, orc = _pair(lambda s: scenes.build_box_pile(s, nx=3, ny=3, nz=3, pitch=0.7, seed=8), **kw)
+    rep = eng.autotune(frames=2)
+    assert rep["chosen"]["mode"] in ("cluster", "grid")
+    eng.step()
+    orc.step()
+    assert np.abs(eng.positions() - orc.positions()).max() <= 1e-5
 
 
 def test_pair_capacity_overflow_grows():

@@ -76,7 +76,7 @@ _SIGS = {
     "xpbd3_step": ([_p, C.c_int, _p], C.c_int),
     "xpbd3_status": ([_p, _ip, _p], C.c_int),
     "xpbd3_launch_info": ([_p, _ip, _ip, _ip], C.c_int),
-    "xpbd3_force_mode": ([_p, C.c_int], C.c_int),
+    "xpbd3_set_driver": ([_p, C.c_int, C.c_int, C.c_int], C.c_int),
     "xpbd_color_constraints": ([C.c_int, C.c_int, _p, _p, _p], C.c_int),
     "xpbd_color_ranges": ([C.c_int, _p, _p, _p], C.c_int),
     "xpbd3_contacts_create": ([C.POINTER(_p), C.c_int, C.c_int], C.c_int),

@@ -53,7 +53,8 @@ XD uint64_t global_ns() {
 }
 
 // ---- bounded grid barrier --------------------------------------------------------
-// Generation-counting barrier for a cooperative launch (all blocks co-resident).
+// Generation-counting barrier for a cooperative launch (all blocks co-resident),
+// or the hardware cluster barrier when the whole grid is one cluster.
 // Every wait gives up after ~2 s of wall time, sets XPBD_ERR_BARRIER_TIMEOUT in
 // the status word and returns; once the bit is set no barrier waits again, so a
 // kernel can never hang on it.  With one block it is a plain __syncthreads().
@@ -61,6 +62,7 @@ struct GridBarrier {
   unsigned* count;  // arrivals at the current barrier
   unsigned* gen;    // generation number
   int* status;
+  int cluster;      // 1: the grid is one thread-block cluster -> hardware cluster barrier
 };
 
 constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;
@@ -68,6 +70,13 @@ constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;
 XD void grid_sync(const GridBarrier& b) {
   if (gridDim.x == 1) {
     __syncthreads();
+    return;
+  }
+  if (b.cluster) {
+    // barrier.cluster: release/acquire at cluster scope (covers global memory
+    // written by every thread of the cluster); a hardware barrier, no spin.
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
     return;
   }
   __syncthreads();

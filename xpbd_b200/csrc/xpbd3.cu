@@ -489,6 +489,9 @@ extern "C" int xpbd3_cap_velocity(const xpbd3_state* s, float max_speed, void* s
 }
 
 // ---- solver handle -------------------------------------------------------------
+// Frame drivers: 0 = cooperative grid (bounded global barrier), 1 = one CTA with
+// the particle state staged in shared memory (block barrier), 2 = one
+// thread-block cluster of up to 16 CTAs (hardware cluster barrier).
 struct xpbd3_solver {
   xpbd3_state st{};
   xpbd3_params par{};
@@ -497,15 +500,15 @@ struct xpbd3_solver {
   unsigned* bar = nullptr;  // [count, gen, status(int)]
   int blocks = 1, threads = 256;
   size_t smem = 0;
-  bool use_smem = false;
-  int force_mode = -1;  // -1 auto, 0 global, 1 shared
+  int mode = 0;
+  int force_mode = -1, force_blocks = 0, force_threads = 0;
 };
 
 static constexpr size_t kSmemMax = 227 * 1024;
 
 template <bool GS, bool SMEM>
 static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream) {
-  GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2)};
+  GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2), h->mode == 2 ? 1 : 0};
   auto kern = k3_frames<GS, SMEM>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(h->blocks);
@@ -513,12 +516,46 @@ static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream) {
   cfg.dynamicSmemBytes = h->smem;
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = h->blocks > 1 ? 1 : 0;
+  if (h->mode == 2) {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = h->blocks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+  } else {
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = h->blocks > 1 ? 1 : 0;
+  }
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   XPBD_CUDA(cudaLaunchKernelEx(&cfg, kern, h->dev, h->p3, frames, gb));
   return XPBD_OK;
+}
+
+// Largest cluster (<= want CTAs of `threads`) that the device can launch.
+template <class K>
+static int fit_cluster(K kern, int want, int threads, size_t smem) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) {
+    set_last_error("cudaFuncSetAttribute", e);
+    return -1;
+  }
+  for (int c = std::min(want, 16); c >= 2; c /= 2) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess && n > 0) return c;
+    cudaGetLastError();
+  }
+  return 1;
 }
 
 template <bool GS, bool SMEM>
@@ -529,11 +566,19 @@ static int configure(xpbd3_solver* h) {
     h->blocks = 1;
     return XPBD_OK;
   }
+  long long work = std::max<long long>(h->st.n_bodies, h->st.row_capacity);
+  if (h->mode == 2) {
+    int want = h->force_blocks > 0 ? h->force_blocks : std::max(2, std::min(16, ceil_div(work, 2 * h->threads)));
+    int c = fit_cluster(kern, want, h->threads, 0);
+    if (c < 0) return XPBD_ERR_CUDA;
+    h->blocks = c;
+    if (c == 1) h->mode = 0;
+    return XPBD_OK;
+  }
   int per_sm = 0;
   XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, h->threads, 0));
   if (per_sm < 1) per_sm = 1;
-  long long work = std::max<long long>(h->st.n_bodies, h->st.row_capacity);
-  int want = ceil_div(work, h->threads);
+  int want = h->force_blocks > 0 ? h->force_blocks : ceil_div(work, h->threads);
   h->blocks = std::max(1, std::min(want, per_sm * num_sms()));
   return XPBD_OK;
 }
@@ -559,10 +604,13 @@ extern "C" int xpbd3_destroy(xpbd3_solver* h) {
   return XPBD_OK;
 }
 
-// Testing hook: force the frame driver (-1 auto, 0 global memory, 1 shared memory).
-extern "C" int xpbd3_force_mode(xpbd3_solver* h, int mode) {
-  if (!h) return XPBD_ERR_BAD_ARG;
+// Frame driver selection (autotuner hook): mode -1 auto, 0 cooperative grid,
+// 1 shared-memory single CTA, 2 cluster; blocks/threads 0 = automatic.
+extern "C" int xpbd3_set_driver(xpbd3_solver* h, int mode, int blocks, int threads) {
+  if (!h || mode < -1 || mode > 2 || blocks < 0 || threads < 0 || threads > 1024 || (threads % 32)) return XPBD_ERR_BAD_ARG;
   h->force_mode = mode;
+  h->force_blocks = blocks;
+  h->force_threads = threads;
   return XPBD_OK;
 }
 
@@ -588,19 +636,23 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   size_t smem = (size_t)s->n_bodies * 4 * sizeof(float4) + (size_t)s->row_capacity * sizeof(float);
   smem = (smem + 15) & ~(size_t)15;
   bool fits = smem <= kSmemMax;
-  h->use_smem = (h->force_mode == 1) ? fits : (h->force_mode == 0 ? false : fits);
-  if (h->use_smem) {
+  long long work = std::max<long long>(s->n_bodies, s->row_capacity);
+  int mode = h->force_mode;
+  if (mode == 1 && !fits) mode = 2;
+  if (mode < 0) mode = fits ? 1 : (work <= 16LL * 1024 * 8 ? 2 : 0);
+  h->mode = mode;
+  if (mode == 1) {
     h->smem = smem;
-    long long work = std::max<long long>(s->n_bodies, s->row_capacity / 4);
-    int t = (int)std::min<long long>(1024, std::max<long long>(128, ((work + 31) / 32) * 32));
-    h->threads = t;
+    long long w = std::max<long long>(s->n_bodies, s->row_capacity / 4);
+    h->threads = h->force_threads > 0 ? h->force_threads
+                                      : (int)std::min<long long>(1024, std::max<long long>(128, ((w + 31) / 32) * 32));
   } else {
     h->smem = 0;
-    h->threads = 256;
+    h->threads = h->force_threads > 0 ? h->force_threads : (mode == 2 ? 1024 : 256);
   }
   int rc;
-  if (p->gs) rc = h->use_smem ? configure<true, true>(h) : configure<true, false>(h);
-  else rc = h->use_smem ? configure<false, true>(h) : configure<false, false>(h);
+  if (p->gs) rc = mode == 1 ? configure<true, true>(h) : configure<true, false>(h);
+  else rc = mode == 1 ? configure<false, true>(h) : configure<false, false>(h);
   return rc;
 }
 
@@ -608,8 +660,9 @@ extern "C" int xpbd3_step(xpbd3_solver* h, int frames, void* stream) {
   if (!h || frames < 0) return XPBD_ERR_BAD_ARG;
   if (frames == 0 || h->st.n_bodies == 0) return XPBD_OK;
   cudaStream_t st = as_stream(stream);
-  if (h->par.gs) return h->use_smem ? launch_frames<true, true>(h, frames, st) : launch_frames<true, false>(h, frames, st);
-  return h->use_smem ? launch_frames<false, true>(h, frames, st) : launch_frames<false, false>(h, frames, st);
+  const bool sm = h->mode == 1;
+  if (h->par.gs) return sm ? launch_frames<true, true>(h, frames, st) : launch_frames<true, false>(h, frames, st);
+  return sm ? launch_frames<false, true>(h, frames, st) : launch_frames<false, false>(h, frames, st);
 }
 
 extern "C" int xpbd3_status(xpbd3_solver* h, int* out, void* stream) {
@@ -623,7 +676,7 @@ extern "C" int xpbd3_status(xpbd3_solver* h, int* out, void* stream) {
 
 extern "C" int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int* smem_bytes) {
   if (!h) return XPBD_ERR_BAD_ARG;
-  if (blocks) *blocks = h->blocks;
+  if (blocks) *blocks = h->mode == 2 ? -h->blocks : h->blocks;
   if (threads) *threads = h->threads;
   if (smem_bytes) *smem_bytes = (int)h->smem;
   return XPBD_OK;

@@ -477,7 +477,7 @@ XD void body_apply_velocity6(const Dev6& s, int i, const Par6& p) {
 
 // ---------------------------------------------------------------------------------
 // Persistent substep kernel: every substep of one frame in one launch.
-__global__ void __launch_bounds__(256) k6_substeps(Dev6 s, Par6 p, GridBarrier bar) {
+__global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier bar) {
   const int n = s.n, nj = s.nj;
   const int np = min(*s.n_pairs, s.cap);
   const int t0 = gtid(), st = gstride();
@@ -1183,6 +1183,8 @@ extern "C" int xpbd6_body_aabb(const xpbd6_state* s, const xpbd6_params* p, floa
 }
 
 // ---- solver handle ------------------------------------------------------------------
+// Substep drivers: 0 = cooperative grid (bounded global barrier), 2 = one
+// thread-block cluster of up to 16 CTAs (hardware cluster barrier).
 struct xpbd6_solver {
   xpbd6_state st{};
   xpbd6_params par{};
@@ -1192,11 +1194,10 @@ struct xpbd6_solver {
   void* buf = nullptr;
   size_t buf_bytes = 0;
   unsigned* bar = nullptr;  // count, gen, status
-  int blocks = 1, threads = 256;
-  int force_blocks = 0;
+  int blocks = 1, threads = 256, mode = 0;
+  int force_mode = -1, force_blocks = 0, force_threads = 0;
   double hg_rsmax = 0.0, hg_cell = 0.0, maxhe = 0.0;
   cudaGraphExec_t graph = nullptr;
-  cudaStream_t graph_stream = nullptr;
 };
 
 static void free_graph(xpbd6_solver* h) {
@@ -1227,10 +1228,14 @@ extern "C" int xpbd6_destroy(xpbd6_solver* h) {
   return XPBD_OK;
 }
 
-// Testing hook: fixed number of blocks for the persistent substep kernel (0 = auto).
-extern "C" int xpbd6_force_blocks(xpbd6_solver* h, int blocks) {
-  if (!h || blocks < 0) return XPBD_ERR_BAD_ARG;
+// Substep driver selection (autotuner hook): mode -1 auto, 0 cooperative grid,
+// 2 cluster; blocks/threads 0 = automatic.
+extern "C" int xpbd6_set_driver(xpbd6_solver* h, int mode, int blocks, int threads) {
+  if (!h || mode < -1 || mode > 2 || mode == 1 || blocks < 0 || threads < 0 || threads > 512 || (threads % 32))
+    return XPBD_ERR_BAD_ARG;
+  h->force_mode = mode;
   h->force_blocks = blocks;
+  h->force_threads = threads;
   return XPBD_OK;
 }
 
@@ -1241,6 +1246,30 @@ extern "C" int xpbd6_set_grid_constants(xpbd6_solver* h, double rs_max, double c
   h->hg_cell = cell;
   h->maxhe = max_he;
   return XPBD_OK;
+}
+
+static int cluster_fit6(int want, int threads) {
+  cudaError_t e = cudaFuncSetAttribute(k6_substeps, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) {
+    set_last_error("cudaFuncSetAttribute", e);
+    return -1;
+  }
+  for (int c = std::min(want, 16); c >= 2; c /= 2) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(threads);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k6_substeps, &cfg) == cudaSuccess && n > 0) return c;
+    cudaGetLastError();
+  }
+  return 1;
 }
 
 extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_params* p) {
@@ -1291,14 +1320,27 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
   q.cval = reinterpret_cast<uint32_t*>(b + o_cv);
   q.red = reinterpret_cast<int*>(b + o_red);
   q.half = reinterpret_cast<float4*>(b + o_half);
-  int per_sm = 0;
-  XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k6_substeps, 256, 0));
-  per_sm = std::max(per_sm, 1);
   long long work = std::max<long long>((long long)s->n_bodies + s->n_joints, s->pair_capacity / 2);
-  int want = std::max(1, ceil_div(work, 256));
-  h->blocks = std::min(want, per_sm * num_sms());
-  if (h->force_blocks > 0) h->blocks = std::min(h->force_blocks, per_sm * num_sms());
-  h->threads = 256;
+  int mode = h->force_mode;
+  if (mode < 0) mode = work <= 16LL * 512 * 16 ? 2 : 0;
+  h->threads = h->force_threads > 0 ? h->force_threads : (mode == 2 ? 512 : 256);
+  if (mode == 2) {
+    int want = h->force_blocks > 0 ? h->force_blocks : std::max(2, std::min(16, ceil_div(work, h->threads)));
+    int c = cluster_fit6(want, h->threads);
+    if (c < 0) return XPBD_ERR_CUDA;
+    if (c >= 2) {
+      h->mode = 2;
+      h->blocks = c;
+      return XPBD_OK;
+    }
+    mode = 0;
+  }
+  h->mode = 0;
+  int per_sm = 0;
+  XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k6_substeps, h->threads, 0));
+  per_sm = std::max(per_sm, 1);
+  int want = std::max(1, ceil_div(work, h->threads));
+  h->blocks = std::min(h->force_blocks > 0 ? h->force_blocks : want, per_sm * num_sms());
   return XPBD_OK;
 }
 
@@ -1356,15 +1398,22 @@ static int run_broadphase(xpbd6_solver* h, cudaStream_t st) {
 
 static int run_substeps(xpbd6_solver* h, cudaStream_t st) {
   if (h->dev.n == 0) return XPBD_OK;
-  GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2)};
+  GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2), h->mode == 2 ? 1 : 0};
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(h->blocks);
   cfg.blockDim = dim3(h->threads);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = h->blocks > 1 ? 1 : 0;
+  if (h->mode == 2) {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = h->blocks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+  } else {
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = h->blocks > 1 ? 1 : 0;
+  }
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   XPBD_CUDA(cudaLaunchKernelEx(&cfg, k6_substeps, h->dev, h->p6, gb));
@@ -1432,7 +1481,7 @@ extern "C" int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream) 
 
 extern "C" int xpbd6_launch_info(xpbd6_solver* h, int* blocks, int* threads) {
   if (!h) return XPBD_ERR_BAD_ARG;
-  if (blocks) *blocks = h->blocks;
+  if (blocks) *blocks = h->mode == 2 ? -h->blocks : h->blocks;
   if (threads) *threads = h->threads;
   return XPBD_OK;
 }

@@ -77,6 +77,7 @@ class Solver:
         self.sync_contacts = True  # read the contact count each frame (exact overflow handling)
         self._n_contacts_host = 0
         self._t = {}
+        self.driver = (-1, 0, 0)  # (mode, blocks, threads): -1 automatic; see set_driver
 
     # ---- scene building (solver.py:130-228) ---------------------------------------
     def add_particle(self, position, mass, velocity=(0.0, 0.0, 0.0), shape: Shape | None = None,
@@ -284,12 +285,32 @@ class Solver:
         p.gs = 1 if self.solve_mode == "gs" else 0
         return p
 
+    def set_driver(self, mode: int = -1, blocks: int = 0, threads: int = 0) -> None:
+        """Frame driver: -1 automatic, 0 cooperative grid, 1 one CTA with the
+        state in shared memory, 2 one thread-block cluster; 0 = automatic size."""
+        self.driver = (int(mode), int(blocks), int(threads))
+        if self._h is not None and not self._dirty:
+            self._bind()
+
+    def launch_info(self) -> dict:
+        self._flush()
+        b, t, sm = C.c_int(), C.c_int(), C.c_int()
+        N.lib().xpbd3_launch_info(self._h, C.byref(b), C.byref(t), C.byref(sm))
+        mode = "cluster" if b.value < 0 else ("shared" if sm.value > 0 else "grid")
+        return {"mode": mode, "blocks": abs(b.value), "threads": t.value, "smem_bytes": sm.value}
+
+    def autotune(self, frames: int = 3, candidates=None) -> dict:
+        """Time the frame drivers on the current scene and keep the fastest."""
+        from .autotune import tune3
+        return tune3(self, frames, candidates)
+
     def _bind(self) -> None:
         L = N.lib()
         if self._h is None:
             h = C.c_void_p()
             N.check(L.xpbd3_create(C.byref(h)), "xpbd3_create")
             self._h = h
+        N.check(L.xpbd3_set_driver(self._h, *[int(v) for v in self.driver]), "xpbd3_set_driver")
         self._st = self._state()
         self._par = self._params()
         N.check(L.xpbd3_bind(self._h, C.byref(self._st), C.byref(self._par)), "xpbd3_bind")

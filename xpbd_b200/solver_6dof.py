@@ -68,7 +68,7 @@ _SIGS6 = {
     "xpbd6_substeps": ([C.c_void_p, C.c_void_p], C.c_int),
     "xpbd6_step": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
     "xpbd6_status": ([C.c_void_p, C.POINTER(C.c_int), C.c_void_p], C.c_int),
-    "xpbd6_force_blocks": ([C.c_void_p, C.c_int], C.c_int),
+    "xpbd6_set_driver": ([C.c_void_p, C.c_int, C.c_int, C.c_int], C.c_int),
     "xpbd6_set_grid_constants": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
     "xpbd6_launch_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "xpbd6_morton": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
@@ -133,7 +133,7 @@ class Solver6DOF:
         self.cap = 0
         self._n_pairs_host = 0
         self.sync_pairs = True
-        self.force_blocks = 0
+        self.driver = (-1, 0, 0)  # (mode, blocks, threads): -1 automatic; see set_driver
 
     # ---- scene building (solver_6dof.py:166-229) ----------------------------------
     def _add_body(self, position, half_extents, mass, quaternion, velocity, omega, color, static,
@@ -291,7 +291,7 @@ class Solver6DOF:
         """solver_6dof.py:481-487: parameters baked into a bound handle / graph."""
         return (self.cap, self.substeps, self.iterations, self.gyroscopic, self.dt, self.gravity, self.floor_y,
                 self.friction, self.restitution, self.lin_damp, self.ang_damp, self.jacobi_relax, self.max_speed,
-                self.max_omega, self._man_margin, self.broadphase, self.force_blocks)
+                self.max_omega, self._man_margin, self.broadphase, self.driver)
 
     def _bind(self):
         L = lib6()
@@ -301,11 +301,30 @@ class Solver6DOF:
             self._h = h
         self._st = self._state()
         self._par = self._params()
-        N.check(L.xpbd6_force_blocks(self._h, int(self.force_blocks)), "xpbd6_force_blocks")
+        N.check(L.xpbd6_set_driver(self._h, *[int(v) for v in self.driver]), "xpbd6_set_driver")
         N.check(L.xpbd6_set_grid_constants(self._h, self._rs_max, self._hg_cell, self._rs_max),
                 "xpbd6_set_grid_constants")
         N.check(L.xpbd6_bind(self._h, C.byref(self._st), C.byref(self._par)), "xpbd6_bind")
         self._sig = self._signature()
+
+    def set_driver(self, mode=-1, blocks=0, threads=0):
+        """Substep driver: -1 automatic, 0 cooperative grid, 2 one thread-block
+        cluster (hardware cluster barrier); blocks/threads 0 = automatic."""
+        self.driver = (int(mode), int(blocks), int(threads))
+        self._sig = None
+
+    def launch_info(self):
+        self._flush()
+        if self._sig != self._signature():
+            self._bind()
+        b, t = C.c_int(), C.c_int()
+        lib6().xpbd6_launch_info(self._h, C.byref(b), C.byref(t))
+        return {"mode": "cluster" if b.value < 0 else "grid", "blocks": abs(b.value), "threads": t.value}
+
+    def autotune(self, frames=3, candidates=None):
+        """Time the substep drivers on the current scene and keep the fastest."""
+        from .autotune import tune6
+        return tune6(self, frames, candidates)
 
     def invalidate(self):
         """Re-bind (and re-capture the frame graph) before the next step."""
