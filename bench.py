@@ -38,6 +38,8 @@ WORKLOADS = {
     "cloth_jacobi": "cloth 32x32 as above, jacobi 15x2",
     "boxes": "box pile 1440 (12x10x12 lattice pitch 0.8 m, half extents U[0.1,0.3] m, density 1000, random "
              "orientation, mu=0.6, e=0.2), LBVH, 15x2",
+    "batch": "256 independent scenes from seed 0: 128 cloths n x n (n ~ U{16..128}, gs, per-scene coloring) + "
+             "128 box piles of k boxes (k ~ U{64..1024}, LBVH), packed into one 3-DOF and one 6-DOF system, 15x2",
 }
 SIX_DOF = {"boxes"}
 BYTES_PER_PROJ = {0: 88, 1: 88, 2: 64, 3: 112}   # DISTANCE, ATTACH, FLOOR, CONTACT (Jacobi)
@@ -141,7 +143,66 @@ def algorithmic_bytes(solver, rows_type_counts, gs):
     return b
 
 
+def time_batch(args, device, flush_buf, clocks=None, n_scenes=256, sample=(0, 1, 2, 3)):
+    """Aggregate projections/s of the batched scenes, plus per-scene residual
+    against the same scenes solved alone (a sample of scenes)."""
+    import numpy as np
+    import torch
+
+    from xpbd_b200.batch import BatchedScenes, batch_specs
+    t0 = time.perf_counter()
+    b = BatchedScenes(batch_specs(n_scenes, seed=0), device=device)
+    build_s = time.perf_counter() - t0
+    tune = b.autotune(frames=2)
+    for _ in range(args.warmup):
+        b.step()
+    torch.cuda.synchronize(device)
+    stream = torch.cuda.current_stream(device)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
+        for k in range(args.steps):
+            if flush_buf is not None:
+                flush_buf.zero_()
+            ev[k][0].record(stream)
+            b.step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(device)
+    frame_ms = [a.elapsed_time(c) for a, c in ev]
+    proj = b.projections_per_frame()
+    res = b.residuals()
+    frames_done = args.warmup + args.steps
+    checks = {}
+    for i in sample:
+        s = b.solo(i)
+        for _ in range(frames_done):
+            s.step()
+        torch.cuda.synchronize(device)
+        d = float(np.abs(b.scene_positions(i) - s.positions()).max())
+        checks[str(i)] = {"kind": b.specs[i].kind, "size": b.specs[i].size, "residual_batched": float(res[i]),
+                          "residual_solo": float(s.residual()[0]), "max_abs_dx_vs_solo": d}
+    S, I = b.cloth.substeps, b.cloth.iterations
+    rows3 = b.cloth.num_constraints
+    n3 = b.cloth.num_bodies
+    alg3 = S * I * rows3 * 84 + S * n3 * BODY_SUBSTEP_BYTES
+    T = b.piles.tensors
+    npairs = min(b.piles.n_pairs, b.piles.cap)
+    pts = int(T["m_hdr"][:npairs, 0].sum().item())
+    n6 = b.piles.num_bodies
+    alg6 = S * (I * (pts * 196 + 8 * n6 * 47) + npairs * 300 + n6 * 128)
+    return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=frame_ms, proj_per_frame=proj,
+                rows=rows3, bodies=n3 + n6, status=b.piles.status() | b.cloth.status(), alg_bytes=alg3 + alg6,
+                launches=args.steps * 17,
+                launch={"cloth": b.cloth.launch_info(), "piles": b.piles.launch_info(), "autotune": tune,
+                        "build_s": round(build_s, 1), "residual_max": float(res.max()),
+                        "residual_median": float(np.median(res)), "vs_solo": checks,
+                        "cloth_particles": n3, "cloth_rows": rows3, "boxes": n6, "pairs": npairs,
+                        "manifold_points": pts})
+
+
 def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
+    if workload == "batch":
+        return time_batch(args, device, flush_buf, clocks)
     if workload in SIX_DOF:
         return time_engine6(args, workload, device, flush_buf, clocks)
     import ctypes as C
@@ -447,13 +508,14 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 5), "peak_kind": peak_kind,
                          "traffic": traffic_for(args.workload),
-                         "kernel": "k6_substeps" if args.workload in SIX_DOF else "k3_frames",
+                         "kernel": {"batch": "k3_frames + k6_substeps (whole frame)"}.get(
+                             args.workload, "k6_substeps" if args.workload in SIX_DOF else "k3_frames"),
                          "kernel_ms": round(kern_ms, 5), "alg_bytes_per_launch": r["alg_bytes"]},
             "gpu_launches": r["launches"],
             "status_bits": r["status"],
         }
         line["clocks"] = clocks.summary()
-        if args.kernels_only:
+        if args.kernels_only or args.workload == "batch":
             print(json.dumps(line), flush=True)
             return
         try:

@@ -110,6 +110,14 @@ int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int* smem_byte
  * cluster (2-16 CTAs, hardware cluster barrier); blocks/threads 0 = automatic. */
 int xpbd3_set_driver(xpbd3_solver* h, int mode, int blocks, int threads);
 
+/* Constraint residual after a solve (no reference counterpart; the metric of
+ * the benchmark and of the learned warm start): hard rows max(0, -C),
+ * compliant rows |C + alpha~ lambda| with alpha~ = compliance / h^2.  Writes the
+ * max per scene to out_scene[n_scenes] (row_scene[m] gives each row's scene;
+ * NULL = one scene) and, if out_rows != NULL, every row's residual. */
+int xpbd3_residual(const xpbd3_state* s, float h, const int* row_scene, int n_scenes, float* out_scene,
+                   float* out_rows, void* stream);
+
 /* coloring.py:26-71 color_constraints (host, Welsh-Powell, bit-exact order).
  * Returns the number of colors, or -1 on bad arguments. */
 int xpbd_color_constraints(int n_bodies, int m, const int* a, const int* b, int* color);
@@ -150,6 +158,27 @@ int xpbd3_contacts_build_noalloc(const xpbd3_state* s, const float* radius, cons
                                  int n_existing, const float* x_init, double contact_margin, double dt,
                                  double r_max, int* status_dev, void* stream);
 
+/* ---- learned lambda warm start (no reference counterpart: the reference always
+ * restarts a substep from lambda = 0, solver.py:430-431) ---------------------------
+ * MLP 7 -> 64 -> 64 -> 1 (GELU), 4737 parameters, bf16 weights, fp32 accumulation. */
+int xpbd_mlp_num_params(void);
+/* Per-row features at the current (just integrated) positions: feats float[cap][8]
+ * (C, w, alpha~, lambda_prev, depth, cos(n, g), v_rel.n, transformed), and
+ * weff = w + alpha~ (0 = row not warm-started). */
+int xpbd3_features(const xpbd3_state* s, float h, float gx, float gy, float gz, float* feats, float* weff,
+                   void* stream);
+/* lambda0[j] = slog^-1(MLP(feats[j])) 1 mm / weff[j] for m rows (bf16 weights). */
+int xpbd_mlp_infer(const float* feats, const float* weff, int m, const void* weights_bf16, float* lam0,
+                   void* stream);
+/* Loss (mean squared error) of a batch and its gradient, added into G. */
+int xpbd_mlp_grads(const float* feats, const float* targets, int B, const void* weights_bf16, float* G,
+                   float* loss, void* stream);
+/* One Adam step on fp32 master weights w (moments M, V); refreshes the bf16 copy, clears G. */
+int xpbd_mlp_adam(float* w, float* G, float* M, float* V, void* weights_bf16, float lr, int step, void* stream);
+/* Seeds lambda := lambda0 and accumulates the Jacobi position correction
+ * M^-1 grad C^T lambda0 into acc (apply with xpbd3_apply_jacobi). */
+int xpbd3_warm_start(const xpbd3_state* s, const float* lam0, void* stream);
+
 /* Device primitives exposed for tests (no reference counterpart): stable sort
  * of uint64 keys with uint32 values, and exclusive scan of int32. */
 int xpbd_sort_pairs_u64(uint64_t* keys, uint32_t* vals, int n, int max_bits, void* stream);
@@ -186,6 +215,8 @@ typedef struct xpbd6_state {
     float* j_anchor_a; /* float4[n_joints]: anchor in A's frame, rest w  */
     float* j_anchor_b; /* float4[n_joints]: anchor in B's frame, compliance w */
     float* lam_joint;  /* float[n_joints]                                */
+    int* scene;        /* int[n] scene id per body (batched independent scenes; NULL = one scene) */
+    int n_scenes;
 } xpbd6_state;
 
 typedef struct xpbd6_params {
@@ -236,6 +267,11 @@ int xpbd6_launch_info(xpbd6_solver* h, int* blocks, int* threads);
 /* Host constants of the hash-grid / grid broad phases (solver_6dof.py:335-337,
  * 244): largest bounding radius |he|, hash-grid cell, largest |he| for the grid margin. */
 int xpbd6_set_grid_constants(xpbd6_solver* h, double rs_max, double cell, double max_he);
+/* Residual after a frame (no reference counterpart): joints |C + alpha~ lambda|,
+ * floor corners and manifold points max(0, -C), max per scene (body_scene[n],
+ * NULL = one scene) into out_scene[n_scenes]. */
+int xpbd6_residual(const xpbd6_state* s, const xpbd6_params* p, const int* body_scene, int n_scenes,
+                   float* out_scene, void* stream);
 /* Morton keys of the LBVH over lowers/uppers (float4[n]) -> uint32[n]. */
 int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream);
 

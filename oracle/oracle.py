@@ -59,6 +59,8 @@ def lib():
         L.or6_pairs_grid.restype = C.c_int64
         L.or3_color_constraints.restype = C.c_int
         L.or3_color_ranges.restype = C.c_int
+        L.or3_residual.restype = C.c_float
+        L.or6_residual.restype = C.c_float
     return _LIB
 
 
@@ -408,6 +410,13 @@ class OracleSolver:
     def velocities(self):
         return self.v.copy() if self.v is not None else _f32(self._v, (-1, 3))
 
+    def residual(self, per_row=False):
+        """Max residual: hard rows max(0, -C), compliant rows |C + alpha~ lambda|."""
+        self._flush()
+        rows = np.zeros(max(len(self._rows), 1), np.float32)
+        mx = lib().or3_residual(C.byref(self._scene()), C.c_float(self.dt / self.substeps), fp(rows))
+        return (float(mx), rows[:len(self._rows)]) if per_row else float(mx)
+
     def lambdas(self):
         return self.lam.copy() if self.lam is not None else np.zeros(len(self._rows), np.float32)
 
@@ -620,6 +629,12 @@ class OracleSolver6DOF:
             return
         self.n_pairs = self._broadphase()
         lib().or6_frame(C.byref(self._scene()), C.byref(self._params()))
+
+    def residual(self):
+        """Max residual of the last frame's joints, floor corners and manifold points."""
+        self._flush()
+        return float(lib().or6_residual(C.byref(self._scene()), C.c_float(self.floor_y),
+                                        C.c_float(self.dt / self.substeps)))
 
     def set_velocity(self, idx, vel):
         self._flush(); self.v[idx] = np.asarray(vel, np.float32)

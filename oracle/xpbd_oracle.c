@@ -1219,3 +1219,179 @@ void or_morton_codes(int n, const float *lo, const float *hi, uint32_t *codes) {
         codes[i] = k;
     }
 }
+
+/* ---------------------------------------------------------------------- */
+/* Constraint residual after a solve (no reference counterpart; the metric the
+ * benchmark reports): hard rows max(0, -C), compliant rows |C + alpha~ lambda|
+ * with alpha~ = compliance / h^2 (XPBD paper Eq. 8).  Rows skipped by the
+ * solver (inactive, both bodies static) contribute 0. */
+float or3_residual(const or3_scene *S, float h, float *per_row) {
+    float inv_dt2 = 1.0f / (h * h), mx = 0.0f;
+    for (int j = 0; j < S->n_rows; ++j) {
+        float res = 0.0f;
+        int t = S->r_type[j];
+        if (S->r_active[j]) {
+            int a = S->r_a[j];
+            float wa = S->inv_mass[a];
+            if (t == DISTANCE || t == ATTACH) {
+                v3 pb; float wb;
+                if (t == ATTACH) { pb = ld3(S->r_anchor + 3 * j); wb = 0.0f; }
+                else { pb = ld3(S->x + 3 * S->r_b[j]); wb = S->inv_mass[S->r_b[j]]; }
+                if (wa + wb != 0.0f) {
+                    float C = len3(sub3(ld3(S->x + 3 * a), pb)) - S->r_rest[j];
+                    float alpha = S->r_comp[j] * inv_dt2;
+                    res = fabsf(C + alpha * S->r_lambda[j]);
+                }
+            } else if (t == FLOOR) {
+                if (wa != 0.0f) {
+                    float C = S->x[3 * a + 1] - S->r_anchor[3 * j + 1];
+                    res = C < 0.0f ? -C : 0.0f;
+                }
+            } else if (t == CONTACT) {
+                int b = S->r_b[j];
+                if (wa + S->inv_mass[b] != 0.0f) {
+                    float C = len3(sub3(ld3(S->x + 3 * a), ld3(S->x + 3 * b))) - S->r_rest[j];
+                    res = C < 0.0f ? -C : 0.0f;
+                }
+            }
+        }
+        if (per_row) per_row[j] = res;
+        if (res > mx) mx = res;
+    }
+    return mx;
+}
+
+float or6_residual(const or6_scene *S, float floor_y, float h) {
+    float mx = 0.0f;
+    for (int k = 0; k < S->n_joints; ++k) {
+        int a = S->j_a[k], b = S->j_b[k];
+        v3 pa = add3(ld3(S->x + 3 * a), qrot(ld4(S->q + 4 * a), ld3(S->j_anchor_a + 3 * k)));
+        v3 pb = add3(ld3(S->x + 3 * b), qrot(ld4(S->q + 4 * b), ld3(S->j_anchor_b + 3 * k)));
+        float C = len3(sub3(pa, pb)) - S->j_rest[k];
+        float r = fabsf(C + (S->j_comp[k] / (h * h)) * S->lam_joint[k]);
+        if (r > mx) mx = r;
+    }
+    for (int i = 0; i < S->n; ++i) {
+        if (S->inv_mass[i] == 0.0f) continue;
+        v3 xi = ld3(S->x + 3 * i), he = ld3(S->he + 3 * i);
+        q4 qi = ld4(S->q + 4 * i);
+        for (int c = 0; c < 8; ++c) {
+            float d = floor_y - add3(xi, qrot(qi, box_corner(he, c))).y;
+            if (d > mx) mx = d;
+        }
+    }
+    for (int pid = 0; pid < S->cap && pid < S->n_pairs; ++pid) {
+        int nc = S->m_count[pid], inc = S->m_inc[pid], ref = S->m_ref[pid];
+        v3 s = ld3(S->m_normal + 3 * pid);
+        for (int c = 0; c < nc; ++c) {
+            int slot = pid * 8 + c;
+            v3 p_inc = add3(ld3(S->x + 3 * inc), qrot(ld4(S->q + 4 * inc), ld3(S->m_off_inc + 3 * slot)));
+            v3 p_ref = add3(ld3(S->x + 3 * ref), qrot(ld4(S->q + 4 * ref), ld3(S->m_off_ref + 3 * slot)));
+            float C = dot3(sub3(p_inc, p_ref), s);
+            if (-C > mx) mx = -C;
+        }
+    }
+    return mx;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Learned warm start MLP (no reference counterpart): 7 -> 64 -> 64 -> 1 with
+ * GELU, weights rounded to bf16 (round to nearest even), fp32 arithmetic with
+ * double-precision sums for the batch reductions.  Mean squared error over the
+ * batch (loss = mean e^2) and its gradient d(0.5 mean e^2)/dw, the quantity
+ * the engine's training kernel accumulates. */
+#define MLP_IN 7
+#define MLP_H 64
+#define MLP_NP (MLP_H * MLP_IN + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1)
+
+float or_bf16_round(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) { u &= 0xffff0000u; memcpy(&x, &u, 4); return x; }
+    uint32_t lsb = (u >> 16) & 1u;
+    u += 0x7fffu + lsb;
+    u &= 0xffff0000u;
+    memcpy(&x, &u, 4);
+    return x;
+}
+
+static float or_gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+static float or_gelu_d(float x) {
+    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+/* feats: B x 8 (first 7 used), targets: B, w: MLP_NP fp32 (rounded to bf16
+ * here), G: MLP_NP output gradient, returns the loss. */
+double or_mlp_grads(const float *feats, const float *targets, int B, const float *w_in, double *G) {
+    float W[MLP_NP];
+    for (int i = 0; i < MLP_NP; ++i) W[i] = or_bf16_round(w_in[i]);
+    const float *W1 = W, *B1 = W1 + MLP_H * MLP_IN, *W2 = B1 + MLP_H, *B2 = W2 + MLP_H * MLP_H, *W3 = B2 + MLP_H,
+                *B3 = W3 + MLP_H;
+    double *G1 = G, *GB1 = G1 + MLP_H * MLP_IN, *G2 = GB1 + MLP_H, *GB2 = G2 + MLP_H * MLP_H, *G3 = GB2 + MLP_H,
+           *GB3 = G3 + MLP_H;
+    memset(G, 0, sizeof(double) * MLP_NP);
+    double loss = 0.0;
+    for (int s = 0; s < B; ++s) {
+        const float *x = feats + 8 * s;
+        float z1[MLP_H], a1[MLP_H], z2[MLP_H], a2[MLP_H];
+        for (int u = 0; u < MLP_H; ++u) {
+            float z = B1[u];
+            for (int k = 0; k < MLP_IN; ++k) z = fmaf(W1[u * MLP_IN + k], x[k], z);
+            z1[u] = z; a1[u] = or_gelu(z);
+        }
+        for (int u = 0; u < MLP_H; ++u) {
+            float z = B2[u];
+            for (int k = 0; k < MLP_H; ++k) z = fmaf(W2[u * MLP_H + k], a1[k], z);
+            z2[u] = z; a2[u] = or_gelu(z);
+        }
+        float y = B3[0];
+        for (int u = 0; u < MLP_H; ++u) y = fmaf(W3[u], a2[u], y);
+        double e = (double)y - (double)targets[s];
+        loss += e * e;
+        double dy = e / (double)B;
+        double dz2[MLP_H], dz1[MLP_H];
+        for (int u = 0; u < MLP_H; ++u) {
+            G3[u] += dy * a2[u];
+            dz2[u] = dy * W3[u] * or_gelu_d(z2[u]);
+        }
+        GB3[0] += dy;
+        for (int u = 0; u < MLP_H; ++u) {
+            for (int k = 0; k < MLP_H; ++k) G2[u * MLP_H + k] += dz2[u] * a1[k];
+            GB2[u] += dz2[u];
+        }
+        for (int k = 0; k < MLP_H; ++k) {
+            double a = 0.0;
+            for (int u = 0; u < MLP_H; ++u) a += (double)W2[u * MLP_H + k] * dz2[u];
+            dz1[k] = a * or_gelu_d(z1[k]);
+        }
+        for (int u = 0; u < MLP_H; ++u) {
+            for (int k = 0; k < MLP_IN; ++k) G1[u * MLP_IN + k] += dz1[u] * x[k];
+            GB1[u] += dz1[u];
+        }
+    }
+    return loss / (double)B;
+}
+
+/* Forward pass only (predicted y per sample). */
+void or_mlp_forward(const float *feats, int B, const float *w_in, float *y_out) {
+    float W[MLP_NP];
+    for (int i = 0; i < MLP_NP; ++i) W[i] = or_bf16_round(w_in[i]);
+    const float *W1 = W, *B1 = W1 + MLP_H * MLP_IN, *W2 = B1 + MLP_H, *B2 = W2 + MLP_H * MLP_H, *W3 = B2 + MLP_H,
+                *B3 = W3 + MLP_H;
+    for (int s = 0; s < B; ++s) {
+        const float *x = feats + 8 * s;
+        float a1[MLP_H];
+        for (int u = 0; u < MLP_H; ++u) {
+            float z = B1[u];
+            for (int k = 0; k < MLP_IN; ++k) z = fmaf(W1[u * MLP_IN + k], x[k], z);
+            a1[u] = or_gelu(z);
+        }
+        float y = B3[0];
+        for (int u = 0; u < MLP_H; ++u) {
+            float z = B2[u];
+            for (int k = 0; k < MLP_H; ++k) z = fmaf(W2[u * MLP_H + k], a1[k], z);
+            y = fmaf(W3[u], or_gelu(z), y);
+        }
+        y_out[s] = y;
+    }
+}

@@ -49,7 +49,8 @@ class xpbd6_state(C.Structure):
                 ("acc_x", _p), ("acc_r", _p), ("acc_v", _p), ("acc_w", _p), ("lam_floor", _p),
                 ("pairs", _p), ("n_pairs", _p), ("m_hdr", _p), ("m_normal", _p),
                 ("m_off_inc", _p), ("m_off_ref", _p), ("lam_pair", _p),
-                ("j_ab", _p), ("j_anchor_a", _p), ("j_anchor_b", _p), ("lam_joint", _p)]
+                ("j_ab", _p), ("j_anchor_a", _p), ("j_anchor_b", _p), ("lam_joint", _p),
+                ("scene", _p), ("n_scenes", C.c_int)]
 
 
 class xpbd6_params(C.Structure):
@@ -85,6 +86,8 @@ _SIGS = {
                               C.c_double, _p, _p], C.c_int),
     "xpbd_sort_pairs_u64": ([_p, _p, C.c_int, C.c_int, _p], C.c_int),
     "xpbd_scan_i32": ([_p, _p, C.c_int, _p, _p], C.c_int),
+    "xpbd3_residual": ([_p, C.c_float, _p, C.c_int, _p, _p, _p], C.c_int),
+    "xpbd6_residual": ([_p, _p, _p, C.c_int, _p, _p], C.c_int),
 }
 
 _LIB = None

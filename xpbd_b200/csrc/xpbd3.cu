@@ -527,7 +527,14 @@ static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream) {
   }
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  XPBD_CUDA(cudaLaunchKernelEx(&cfg, kern, h->dev, h->p3, frames, gb));
+  cudaError_t e = cudaLaunchKernelEx(&cfg, kern, h->dev, h->p3, frames, gb);
+  if (e != cudaSuccess) {
+    char what[160];
+    snprintf(what, sizeof(what), "k3_frames launch (mode %d, grid %d, block %d, smem %zu, colors %d)", h->mode,
+             h->blocks, h->threads, h->smem, h->dev.ncolors);
+    set_last_error(what, e);
+    return XPBD_ERR_CUDA;
+  }
   return XPBD_OK;
 }
 
@@ -562,7 +569,10 @@ template <bool GS, bool SMEM>
 static int configure(xpbd3_solver* h) {
   auto kern = k3_frames<GS, SMEM>;
   if (SMEM) {
-    XPBD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem));
+    // The attribute is per function, shared by every handle: raise it to the
+    // device maximum rather than to this scene's size, so binding a smaller
+    // scene never lowers the limit another handle's launches rely on.
+    XPBD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
     h->blocks = 1;
     return XPBD_OK;
   }
@@ -679,5 +689,56 @@ extern "C" int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int
   if (blocks) *blocks = h->mode == 2 ? -h->blocks : h->blocks;
   if (threads) *threads = h->threads;
   if (smem_bytes) *smem_bytes = (int)h->smem;
+  return XPBD_OK;
+}
+
+// =============================================================================
+// Residual metric (no reference counterpart): per row, hard rows max(0, -C),
+// compliant rows |C + alpha~ lambda| (XPBD Eq. 8), reduced to a max per scene.
+// =============================================================================
+namespace xpbd {
+__global__ void k3_residual(Dev3 s, float h, const int* row_scene, float* out_scene, float* out_rows) {
+  const int m = *s.n_rows;
+  const float inv_dt2 = 1.0f / (h * h);
+  for (int j = gtid(); j < m; j += gstride()) {
+    int4 r = s.ri[j];
+    float res = 0.0f;
+    if (r.w != 0) {
+      float4 xa = s.x[r.y];
+      float4 f = s.rf[j];
+      if (r.x == XPBD_DISTANCE || r.x == XPBD_ATTACH) {
+        float4 pb = r.x == XPBD_ATTACH ? s.ra[j] : s.x[r.z];
+        float wb = r.x == XPBD_ATTACH ? 0.0f : pb.w;
+        if (xa.w + wb != 0.0f) {
+          float C = length(v3(xa) - v3(pb)) - f.x;
+          res = fabsf(C + (f.y * inv_dt2) * s.lam[j]);
+        }
+      } else if (r.x == XPBD_FLOOR) {
+        if (xa.w != 0.0f) {
+          float C = xa.y - f.w;
+          res = C < 0.0f ? -C : 0.0f;
+        }
+      } else if (r.x == XPBD_CONTACT) {
+        float4 xb = s.x[r.z];
+        if (xa.w + xb.w != 0.0f) {
+          float C = length(v3(xa) - v3(xb)) - f.x;
+          res = C < 0.0f ? -C : 0.0f;
+        }
+      }
+    }
+    if (out_rows) out_rows[j] = res;
+    atomicMax(reinterpret_cast<int*>(out_scene + (row_scene ? row_scene[j] : 0)), __float_as_int(res));
+  }
+}
+}  // namespace xpbd
+
+extern "C" int xpbd3_residual(const xpbd3_state* s, float h, const int* row_scene, int n_scenes, float* out_scene,
+                              float* out_rows, void* stream) {
+  if (check_state(s) || !out_scene || n_scenes < 1) return XPBD_ERR_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  XPBD_CUDA(cudaMemsetAsync(out_scene, 0, sizeof(float) * (size_t)n_scenes, st));
+  if (s->row_capacity == 0) return XPBD_OK;
+  k3_residual<<<stream_blocks(s->row_capacity, 256), 256, 0, st>>>(make_dev3(s), h, row_scene, out_scene, out_rows);
+  XPBD_LAUNCHED();
   return XPBD_OK;
 }

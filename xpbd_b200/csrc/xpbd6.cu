@@ -36,7 +36,8 @@ struct Dev6 {
   const float4* j_a;  // anchor in A's frame, rest in w
   const float4* j_b;  // anchor in B's frame, compliance in w
   float* lam_joint;
-  int n, nj, cap;
+  const int* scene;  // per body (NULL: one scene)
+  int n, nj, cap, n_scenes;
 };
 
 struct Par6 {
@@ -587,6 +588,7 @@ struct BP6 {
   uint32_t* cval;      // n
   int* red;            // 16 ints of reductions
   float4* half;        // n world AABB half extents (grid)
+  int* roots;          // n_scenes: subtree root of each scene in the LBVH (-1: empty scene)
 };
 
 XD int ord_f(float f) {
@@ -658,7 +660,7 @@ XD uint32_t quant10(float t) {
 // The LBVH key: AABB centre normalised to the bounds of all centres, 10 bits
 // per axis, interleaved x-major.  Same definition as the oracle's
 // or_morton_codes.
-__global__ void k6_morton(int n, BP6 b) {
+__global__ void k6_morton(int n, BP6 b, const int* scene) {
   float cmin[3], inv[3];
   for (int d = 0; d < 3; ++d) {
     cmin[d] = unord_f(b.bounds[d]);
@@ -670,22 +672,35 @@ __global__ void k6_morton(int n, BP6 b) {
     float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
     uint32_t k = 0;
     for (int d = 0; d < 3; ++d) k |= expand10(quant10((c[d] - cmin[d]) * inv[d])) << (2 - d);
-    b.keys[i] = k;
+    // batched scenes: the scene id above the 30 Morton bits makes every scene
+    // one contiguous key range, hence one subtree of the radix tree
+    b.keys[i] = scene ? (((uint64_t)scene[i] << 30) | k) : (uint64_t)k;
     b.vals[i] = (uint32_t)i;
   }
 }
 
 XD int lbvh_delta(const uint64_t* k, int n, int i, int j) {
   if (j < 0 || j >= n) return -1;
-  uint32_t a = (uint32_t)k[i], c = (uint32_t)k[j];
-  if (a == c) return 32 + __clz(i ^ j);
-  return __clz(a ^ c);
+  uint64_t a = k[i], c = k[j];
+  if (a == c) return 64 + __clz(i ^ j);
+  return __clzll((long long)(a ^ c));
 }
 
 // Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees
 // and k-d trees", Algorithm 3: internal node i of the radix tree over sorted
 // keys (duplicates broken by index).  Internal nodes 0..n-2, leaf k = n-1+k.
-__global__ void k6_build(int n, BP6 b) {
+XD int scene_at(const BP6& b, const int* scene, int k) { return scene ? scene[b.vals[k]] : 0; }
+
+// A node is the root of scene s when its leaf range is exactly the leaves of s.
+XD void mark_root(const BP6& b, const int* scene, int n, int lo, int hi, int node) {
+  int s = scene_at(b, scene, lo);
+  if (scene_at(b, scene, hi) != s) return;
+  if (lo > 0 && scene_at(b, scene, lo - 1) == s) return;
+  if (hi < n - 1 && scene_at(b, scene, hi + 1) == s) return;
+  b.roots[s] = node;
+}
+
+__global__ void k6_build(int n, BP6 b, const int* scene) {
   for (int i = gtid(); i < n - 1; i += gstride()) {
     const uint64_t* k = b.keys;
     int d = (lbvh_delta(k, n, i, i + 1) - lbvh_delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
@@ -711,19 +726,29 @@ __global__ void k6_build(int n, BP6 b) {
     b.parent[right] = i;
     b.flags[i] = 0;
     if (i == 0) b.parent[0] = -1;
+    mark_root(b, scene, n, min(i, j), max(i, j), i);
   }
 }
 
 // Bottom-up bounds: the second child to arrive at a node writes its union.
-__global__ void k6_refit(int n, BP6 b) {
+// The radix tree over 64-bit keys with the index tie-break is at most 96 levels
+// deep; a walk longer than that means a malformed tree: flag it and stop.
+constexpr int kMaxDepth = 128;
+
+__global__ void k6_refit(int n, BP6 b, const int* scene, int* status) {
   for (int k = gtid(); k < n; k += gstride()) {
     int node = n - 1 + k;
+    mark_root(b, scene, n, k, k, node);  // single-body scenes
     int body = (int)b.vals[k];
     b.nlo[node] = b.lo[body];
     b.nhi[node] = b.hi[body];
     __threadfence();
     int cur = b.parent[node];
-    while (cur >= 0) {
+    for (int depth = 0; cur >= 0; ++depth) {
+      if (depth >= kMaxDepth || cur >= n - 1) {
+        raise_status(status, XPBD_ERR_BAD_INDEX);
+        break;
+      }
       if (atomicAdd(&b.flags[cur], 1) == 0) break;
       __threadfence();
       int2 c = b.child[cur];
@@ -743,6 +768,7 @@ XD bool overlaps(float4 alo, float4 ahi, float4 blo, float4 bhi) {
 
 XD bool keep_pair(const Dev6& s, int i, int j) {
   if (!(j > i)) return false;
+  if (s.scene && s.scene[i] != s.scene[j]) return false;
   if (s.x[i].w == 0.0f && s.x[j].w == 0.0f) return false;
   int gi = s.group[i];
   if (gi == s.group[j] && gi > 0) return false;
@@ -759,12 +785,22 @@ XD void lbvh_query(const Dev6& s, const BP6& b, int i, int* status, Emit emit) {
   float4 qlo = b.lo[i], qhi = b.hi[i];
   int stack[kStack];
   int sp = 0;
-  int node = 0;
-  while (true) {
+  int node = s.scene ? b.roots[s.scene[i]] : 0;
+  if (node < 0 || node >= n - 1) return;  // scene of one body (or empty): no pairs
+  // each internal node is visited at most once in a well-formed tree
+  for (int visits = 0;; ++visits) {
+    if (visits >= n || node < 0 || node >= n - 1) {
+      raise_status(status, XPBD_ERR_BAD_INDEX);
+      return;
+    }
     int2 c = b.child[node];
     int ch[2] = {c.x, c.y};
     for (int e = 0; e < 2; ++e) {
       int x = ch[e];
+      if (x < 0 || x >= 2 * n - 1) {
+        raise_status(status, XPBD_ERR_BAD_INDEX);
+        continue;
+      }
       if (!overlaps(qlo, qhi, b.nlo[x], b.nhi[x])) continue;
       if (x >= n - 1) {
         int j = (int)b.vals[x - (n - 1)];
@@ -1033,6 +1069,7 @@ XD int grid_slot(const Dev6& s, const BP6& b, int o, int k, float margin_f, int6
     if (!(fabsf(xa.y - xb.y) - (ha.y + hb.y + margin_f) <= 0.0f)) continue;
     if (!(fabsf(xa.z - xb.z) - (ha.z + hb.z + margin_f) <= 0.0f)) continue;
     if (!(xa.w > 0.0f || xb.w > 0.0f)) continue;
+    if (s.scene && s.scene[k] != s.scene[partner]) continue;
     int ga = s.group[k];
     if (ga == s.group[partner] && ga > 0) continue;
     emit(cnt, partner);
@@ -1101,6 +1138,8 @@ static Dev6 make_dev6(const xpbd6_state* s) {
   d.j_a = reinterpret_cast<const float4*>(s->j_anchor_a);
   d.j_b = reinterpret_cast<const float4*>(s->j_anchor_b);
   d.lam_joint = s->lam_joint;
+  d.scene = s->scene;
+  d.n_scenes = s->scene ? std::max(s->n_scenes, 1) : 1;
   d.n = s->n_bodies;
   d.nj = s->n_joints;
   d.cap = s->pair_capacity;
@@ -1292,7 +1331,8 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
          o_par = take(4 * 2 * (size_t)n), o_nlo = take(16 * 2 * (size_t)n), o_nhi = take(16 * 2 * (size_t)n),
          o_fl = take(4 * (size_t)n), o_cnt = take(4 * 14 * (size_t)n), o_off = take(4 * 14 * (size_t)n),
          o_sc = take(scan_scratch_bytes(14 * n)), o_cell = take(16 * (size_t)n), o_ck = take(8 * (size_t)n),
-         o_cv = take(4 * (size_t)n), o_red = take(64), o_half = take(16 * (size_t)n);
+         o_cv = take(4 * (size_t)n), o_red = take(64), o_half = take(16 * (size_t)n),
+         o_roots = take(4 * (size_t)std::max(s->scene ? s->n_scenes : 1, 1));
   if (off > h->buf_bytes) {
     if (h->buf) cudaFree(h->buf);
     h->buf = nullptr;
@@ -1320,6 +1360,7 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
   q.cval = reinterpret_cast<uint32_t*>(b + o_cv);
   q.red = reinterpret_cast<int*>(b + o_red);
   q.half = reinterpret_cast<float4*>(b + o_half);
+  q.roots = reinterpret_cast<int*>(b + o_roots);
   long long work = std::max<long long>((long long)s->n_bodies + s->n_joints, s->pair_capacity / 2);
   int mode = h->force_mode;
   if (mode < 0) mode = work <= 16LL * 512 * 16 ? 2 : 0;
@@ -1357,12 +1398,15 @@ static int run_broadphase(xpbd6_solver* h, cudaStream_t st) {
   int rc;
   if (h->par.broadphase == 0) {
     k6_bp_init<<<1, 32, 0, st>>>(b);
+    if (s.scene) XPBD_CUDA(cudaMemsetAsync(b.roots, 0xff, sizeof(int) * (size_t)s.n_scenes, st));
     k6_aabb<<<blocks, 256, 0, st>>>(s, h->p6, b);
-    k6_morton<<<blocks, 256, 0, st>>>(n, b);
+    k6_morton<<<blocks, 256, 0, st>>>(n, b, s.scene);
     XPBD_LAUNCHED();
-    if ((rc = sort_pairs_u64(b.keys, b.vals, n, b.sort_tmp, 30, st))) return rc;
-    k6_build<<<stream_blocks(n - 1, 256), 256, 0, st>>>(n, b);
-    k6_refit<<<blocks, 256, 0, st>>>(n, b);
+    int bits = 30;
+    if (s.scene) for (int ns = s.n_scenes - 1; ns > 0; ns >>= 1) ++bits;
+    if ((rc = sort_pairs_u64(b.keys, b.vals, n, b.sort_tmp, bits, st))) return rc;
+    k6_build<<<stream_blocks(n - 1, 256), 256, 0, st>>>(n, b, s.scene);
+    k6_refit<<<blocks, 256, 0, st>>>(n, b, s.scene, status);
     k6_pairs_count<<<blocks, 256, 0, st>>>(s, b, status);
     XPBD_LAUNCHED();
     if ((rc = exclusive_scan_i32(b.counts, b.offsets, n, s.n_pairs, b.scan_tmp, st))) return rc;
@@ -1470,7 +1514,7 @@ extern "C" int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream) 
   if (n == 0) return XPBD_OK;
   k6_bp_init<<<1, 32, 0, st>>>(h->bp);
   k6_aabb<<<stream_blocks(n, 256), 256, 0, st>>>(h->dev, h->p6, h->bp);
-  k6_morton<<<stream_blocks(n, 256), 256, 0, st>>>(n, h->bp);
+  k6_morton<<<stream_blocks(n, 256), 256, 0, st>>>(n, h->bp, nullptr);
   XPBD_LAUNCHED();
   std::vector<uint64_t> k(n);
   XPBD_CUDA(cudaMemcpyAsync(k.data(), h->bp.keys, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
@@ -1483,5 +1527,62 @@ extern "C" int xpbd6_launch_info(xpbd6_solver* h, int* blocks, int* threads) {
   if (!h) return XPBD_ERR_BAD_ARG;
   if (blocks) *blocks = h->mode == 2 ? -h->blocks : h->blocks;
   if (threads) *threads = h->threads;
+  return XPBD_OK;
+}
+
+// =============================================================================
+// Residual metric (no reference counterpart): joints |C + alpha~ lambda|, floor
+// corners and manifold points max(0, -C), reduced to a max per scene (scene of
+// the joint's first body, of the floor body, of the incident body).
+// =============================================================================
+namespace xpbd {
+XD void max_into(float* out, int scene, float v) { atomicMax(reinterpret_cast<int*>(out + scene), __float_as_int(v)); }
+
+__global__ void k6_residual(Dev6 s, Par6 p, const int* body_scene, float* out) {
+  const int np = min(*s.n_pairs, s.cap);
+  const int work = s.nj + s.n + np;
+  for (int t = gtid(); t < work; t += gstride()) {
+    if (t < s.nj) {
+      int2 ab = s.j_ab[t];
+      float4 ja = s.j_a[t], jb = s.j_b[t];
+      V3 pa = v3(s.x[ab.x]) + qrot(q4(s.q[ab.x]), v3(ja));
+      V3 pb = v3(s.x[ab.y]) + qrot(q4(s.q[ab.y]), v3(jb));
+      float C = length(pa - pb) - ja.w;
+      max_into(out, body_scene ? body_scene[ab.x] : 0, fabsf(C + (jb.w / (p.h * p.h)) * s.lam_joint[t]));
+    } else if (t < s.nj + s.n) {
+      int i = t - s.nj;
+      float4 x4 = s.x[i];
+      if (x4.w == 0.0f) continue;
+      V3 he = v3(s.he[i]);
+      Q4 qi = q4(s.q[i]);
+      float mx = 0.0f;
+      for (int c = 0; c < 8; ++c) mx = fmaxf(mx, p.floor_y - (v3(x4) + qrot(qi, box_corner(he, c))).y);
+      max_into(out, body_scene ? body_scene[i] : 0, mx);
+    } else {
+      int pid = t - s.nj - s.n;
+      int4 hdr = s.m_hdr[pid];
+      V3 S = v3(s.m_normal[pid]);
+      float mx = 0.0f;
+      for (int c = 0; c < hdr.x; ++c) {
+        int slot = 8 * pid + c;
+        V3 p_inc = v3(s.x[hdr.y]) + qrot(q4(s.q[hdr.y]), v3(s.m_off_inc[slot]));
+        V3 p_ref = v3(s.x[hdr.z]) + qrot(q4(s.q[hdr.z]), v3(s.m_off_ref[slot]));
+        mx = fmaxf(mx, -dot(p_inc - p_ref, S));
+      }
+      if (hdr.x) max_into(out, body_scene ? body_scene[hdr.y] : 0, mx);
+    }
+  }
+}
+}  // namespace xpbd
+
+extern "C" int xpbd6_residual(const xpbd6_state* s, const xpbd6_params* p, const int* body_scene, int n_scenes,
+                              float* out_scene, void* stream) {
+  if (check6(s) || !p || !out_scene || n_scenes < 1) return XPBD_ERR_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  XPBD_CUDA(cudaMemsetAsync(out_scene, 0, sizeof(float) * (size_t)n_scenes, st));
+  long long work = (long long)s->n_joints + s->n_bodies + s->pair_capacity;
+  if (work == 0) return XPBD_OK;
+  k6_residual<<<stream_blocks(work, 256), 256, 0, st>>>(make_dev6(s), make_par6(p), body_scene, out_scene);
+  XPBD_LAUNCHED();
   return XPBD_OK;
 }

@@ -78,6 +78,10 @@ class Solver:
         self._n_contacts_host = 0
         self._t = {}
         self.driver = (-1, 0, 0)  # (mode, blocks, threads): -1 automatic; see set_driver
+        # Row ranges colored independently (batched independent scenes): each
+        # scene gets the colors it would get alone, so Gauss-Seidel per scene is
+        # the same computation as solving that scene alone.
+        self.color_groups: list[tuple[int, int]] | None = None
 
     # ---- scene building (solver.py:130-228) ---------------------------------------
     def add_particle(self, position, mass, velocity=(0.0, 0.0, 0.0), shape: Shape | None = None,
@@ -187,12 +191,20 @@ class Solver:
         row_i = np.zeros((max(cap, 1), 4), np.int32)
         row_f = np.zeros((max(cap, 1), 4), np.float32)
         row_a = np.zeros((max(cap, 1), 4), np.float32)
-        for j, r in enumerate(self._rows):
-            if not (0 <= r.body_a < n) or not (-1 <= r.body_b < n) or (r.type in (DISTANCE, CONTACT) and r.body_b < 0):
-                raise IndexError(f"constraint row {j} references a body outside [0, {n})")
-            row_i[j] = (r.type, r.body_a, r.body_b, 1)
-            row_f[j] = (r.rest, r.compliance, r.mu, r.anchor[1])
-            row_a[j, :3] = r.anchor
+        if ms:
+            R = self._rows
+            ti = np.fromiter((v for r in R for v in (r.type, r.body_a, r.body_b)), np.int64, 3 * ms).reshape(ms, 3)
+            tf = np.fromiter((v for r in R for v in (r.rest, r.compliance, r.mu)), np.float64, 3 * ms).reshape(ms, 3)
+            an = np.fromiter((v for r in R for v in r.anchor), np.float64, 3 * ms).reshape(ms, 3)
+            bad = (ti[:, 1] < 0) | (ti[:, 1] >= n) | (ti[:, 2] < -1) | (ti[:, 2] >= n) | (
+                np.isin(ti[:, 0], (DISTANCE, CONTACT)) & (ti[:, 2] < 0))
+            if bad.any():
+                raise IndexError(f"constraint row {int(np.nonzero(bad)[0][0])} references a body outside [0, {n})")
+            row_i[:ms, :3] = ti
+            row_i[:ms, 3] = 1
+            row_f[:ms, :3] = tf
+            row_f[:ms, 3] = an[:, 1]
+            row_a[:ms, :3] = an
         T = {}
         T["x"] = torch.from_numpy(x).to(dev)
         T["v"] = torch.from_numpy(v).to(dev)
@@ -246,11 +258,23 @@ class Solver:
         m = len(a)
         color = np.zeros(max(m, 1), np.int32)
         k = 0
-        if m:
-            k = N.lib().xpbd_color_constraints(len(self._x), m, a.ctypes.data_as(C.c_void_p),
-                                               b.ctypes.data_as(C.c_void_p), color.ctypes.data_as(C.c_void_p))
-            if k < 0:
+        groups = self.color_groups if (self.color_groups and contacts is None) else [(0, m)]
+        for g0, g1 in groups:
+            if g1 <= g0:
+                continue
+            ga = a[g0:g1]
+            gb = b[g0:g1]
+            lo = int(ga.min())
+            hi = int(max(ga.max(), gb.max()))
+            ga = np.ascontiguousarray(ga - lo, dtype=np.int32)  # scene-local body ids
+            gb = np.ascontiguousarray(np.where(gb >= 0, gb - lo, -1), dtype=np.int32)
+            gc = np.zeros(g1 - g0, np.int32)
+            kg = N.lib().xpbd_color_constraints(hi - lo + 1, g1 - g0, ga.ctypes.data_as(C.c_void_p),
+                                                gb.ctypes.data_as(C.c_void_p), gc.ctypes.data_as(C.c_void_p))
+            if kg < 0:
                 raise N.XpbdError("coloring failed (row references a body out of range)")
+            color[g0:g1] = gc
+            k = max(k, kg)
         order = np.zeros(max(m, 1), np.int32)
         starts = np.zeros(k + 1, np.int32)
         if m:
@@ -401,6 +425,21 @@ class Solver:
         s = int(self._t["status"].item())
         self._t["status"].zero_()
         return int(out.value) | s
+
+    def residual(self, row_scene=None, n_scenes: int = 1, per_row: bool = False):
+        """Max constraint residual of the current state (hard rows max(0, -C),
+        compliant rows |C + alpha~ lambda|), per scene when `row_scene` (a device
+        int tensor, one scene id per row) is given."""
+        self._flush()
+        h = self.dt / self.substeps
+        out = torch.zeros(max(int(n_scenes), 1), dtype=torch.float32, device=self.device)
+        rows = torch.zeros(self._cap, dtype=torch.float32, device=self.device) if per_row else None
+        N.check(N.lib().xpbd3_residual(C.byref(self._st), float(h), N.ptr(row_scene), int(n_scenes), N.ptr(out),
+                                       N.ptr(rows), N.stream_of(self.device)), "xpbd3_residual")
+        res = out.cpu().numpy()
+        if per_row:
+            return res, rows[: int(self._t["n_rows"].item())].cpu().numpy()
+        return res
 
     def state_dict(self) -> dict:
         self._flush()

@@ -80,6 +80,7 @@ _SIGS6 = {
     "xpbd6_solve_velocities": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "xpbd6_apply_velocity": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "xpbd6_body_aabb": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "xpbd6_residual": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
 }
 
 
@@ -123,6 +124,7 @@ class Solver6DOF:
         self._man_margin = self.MAN_MARGIN
         self._x, self._q, self._v, self._w = [], [], [], []
         self._inv_mass, self._inv_I, self._he, self._group = [], [], [], []
+        self._scene: list[int] = []  # independent-scene id per body (batched scenes)
         self.bodies: list[RigidBody] = []
         self._j_a, self._j_b, self._j_anchor_a, self._j_anchor_b = [], [], [], []
         self._j_rest, self._j_compliance = [], []
@@ -134,6 +136,7 @@ class Solver6DOF:
         self._n_pairs_host = 0
         self.sync_pairs = True
         self.driver = (-1, 0, 0)  # (mode, blocks, threads): -1 automatic; see set_driver
+        self._scene_default = 0
 
     # ---- scene building (solver_6dof.py:166-229) ----------------------------------
     def _add_body(self, position, half_extents, mass, quaternion, velocity, omega, color, static,
@@ -156,6 +159,7 @@ class Solver6DOF:
             self._inv_I.append(_box_inv_inertia(he, float(mass)))
         self._he.append(he)
         self._group.append(int(group))
+        self._scene.append(self._scene_default)
         self._dirty = True
         rb = RigidBody(index=idx, half_extents=he, color=color, static=static, is_particle=is_particle,
                        group=int(group))
@@ -171,6 +175,12 @@ class Solver6DOF:
                      static=False, group=1):
         return self._add_body(position, (radius, radius, radius), mass, (0.0, 0.0, 0.0, 1.0), velocity,
                               (0.0, 0.0, 0.0), color, static, is_particle=True, group=group)
+
+    def begin_scene(self, scene_id: int) -> None:
+        """Bodies added from now on belong to independent scene `scene_id`: they
+        only collide with bodies of the same scene (batched scenes in one solver)."""
+        self._scene_default = int(scene_id)
+        self._dirty = True
 
     def add_joint(self, a, b, compliance=0.0, rest_length=None, anchor_a=(0.0, 0.0, 0.0),
                   anchor_b=(0.0, 0.0, 0.0)):
@@ -248,6 +258,9 @@ class Solver6DOF:
         T["j_anchor_a"] = f4(self._j_anchor_a, self._j_rest)
         T["j_anchor_b"] = f4(self._j_anchor_b, self._j_compliance)
         T["lam_joint"] = torch.zeros(max(nj, 1), dtype=torch.float32, device=dev)
+        self.n_scenes = (max(self._scene) + 1) if self._scene else 1
+        T["scene"] = (torch.tensor(np.asarray(self._scene, np.int32), device=dev) if self.n_scenes > 1
+                      else torch.zeros(0, dtype=torch.int32, device=dev))
         # graph mode has no per-frame host check, so it starts with more headroom
         self._alloc_pairs(max(64, n * (4 if self.sync_pairs else 16)))
         he = np.asarray(self._he, np.float32).reshape(-1, 3)
@@ -266,6 +279,8 @@ class Solver6DOF:
                   "acc_w", "lam_floor", "pairs", "n_pairs", "m_hdr", "m_normal", "m_off_inc", "m_off_ref",
                   "lam_pair", "j_ab", "j_anchor_a", "j_anchor_b", "lam_joint"):
             setattr(s, f, N.ptr(T[f]))
+        s.scene = N.ptr(T["scene"])
+        s.n_scenes = int(self.n_scenes)
         return s
 
     def _params(self):
@@ -407,6 +422,16 @@ class Solver6DOF:
         out = C.c_int(0)
         N.check(lib6().xpbd6_status(self._h, C.byref(out), N.stream_of(self.device)), "xpbd6_status")
         return int(out.value)
+
+    def residual(self, body_scene=None, n_scenes=1):
+        """Max residual of the last frame's constraints (joints |C + alpha~ lambda|,
+        floor corners and manifold points max(0, -C)), per scene when
+        `body_scene` (device int tensor, one scene id per body) is given."""
+        self._flush()
+        out = torch.zeros(max(int(n_scenes), 1), dtype=torch.float32, device=self.device)
+        N.check(lib6().xpbd6_residual(C.byref(self._st), C.byref(self._par), N.ptr(body_scene), int(n_scenes),
+                                      N.ptr(out), N.stream_of(self.device)), "xpbd6_residual")
+        return out.cpu().numpy()
 
     def state_dict(self):
         self._flush()
