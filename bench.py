@@ -153,9 +153,9 @@ def time_batch(args, device, flush_buf, clocks=None, n_scenes=256, sample=(0, 1,
     t0 = time.perf_counter()
     b = BatchedScenes(batch_specs(n_scenes, seed=0), device=device)
     build_s = time.perf_counter() - t0
-    tune = b.autotune(frames=2)
     for _ in range(args.warmup):
         b.step()
+    tune = b.autotune(frames=2)  # on the warmed-up state (contacts present), restored afterwards
     torch.cuda.synchronize(device)
     stream = torch.cuda.current_stream(device)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -227,9 +227,9 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
         N.check(L.xpbd3_step(s._h, 1, sp), "xpbd3_step")
 
     s._flush()
-    tune = s.autotune(frames=3)
     for _ in range(args.warmup):
         frame()
+    tune = s.autotune(frames=3)  # on the warmed-up state (contacts present), restored afterwards
     torch.cuda.synchronize(device)
     if world > 1:
         import torch.distributed as dist
@@ -285,11 +285,9 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
     L = lib6()
     stream = torch.cuda.current_stream(device)
     sp = N.stream_of(device)
-    for _ in range(3):   # let the pile develop contacts before tuning
-        N.check(L.xpbd6_step(s._h, 1, sp))
-    tune = s.autotune(frames=3)
     for _ in range(args.warmup):
         N.check(L.xpbd6_step(s._h, 1, sp))
+    tune = s.autotune(frames=3)  # on the warmed-up state (contacts present), restored afterwards
     torch.cuda.synchronize(device)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]

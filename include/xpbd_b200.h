@@ -262,6 +262,11 @@ int xpbd6_status(xpbd6_solver* h, int* out, void* stream);
 /* Substep driver for the next bind (no reference counterpart): mode -1
  * automatic, 0 cooperative grid, 2 one thread-block cluster. */
 int xpbd6_set_driver(xpbd6_solver* h, int mode, int blocks, int threads);
+/* Phase granularity for the next bind (no reference counterpart): 8 = eight
+ * lanes per floor body / contact pair / manifold (default), 1 = one thread each. */
+int xpbd6_set_lanes(xpbd6_solver* h, int lanes);
+/* generate_box_manifold (kernels_6dof.py:234-382) with eight lanes per pair. */
+int xpbd6_manifold8(const xpbd6_state* s, float margin, void* stream);
 /* blocks (negative = cluster of that many CTAs) and threads of the substep kernel. */
 int xpbd6_launch_info(xpbd6_solver* h, int* blocks, int* threads);
 /* Host constants of the hash-grid / grid broad phases (solver_6dof.py:335-337,

@@ -57,22 +57,25 @@ def test_mlp_inference_matches_oracle():
     np.testing.assert_allclose(lam0.cpu().numpy(), ref, rtol=1e-4, atol=1e-9)
 
 
-def _cloth(res=24, compliance=1e-6):
+def _cloth(res=32, compliance=1e-5):
+    """A hanging 32 x 32 cloth (spacing 0.02 m, 0.01 kg) at a compliance where
+    the plain Jacobi solve does reach 1e-4 m, slowly (a stiffer cloth never
+    reaches it within the iteration cap from any start)."""
     s = Solver(dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi")
-    scenes.build_cloth(s, res=res, spacing=0.04, y=1.0, compliance=compliance, floor=False)
+    scenes.build_cloth(s, res=res, spacing=0.02, mass=0.01, y=1.0, compliance=compliance, floor=False)
     return s
 
 
 def test_training_lowers_loss_and_warm_start_saves_iterations():
     torch.manual_seed(0)
     s = _cloth()
-    for _ in range(10):  # let the cloth start to hang
+    for _ in range(20):  # let the cloth start to hang
         s.step()
-    F, T = collect(s, substeps=40, iters=50)
+    F, T = collect(s, substeps=30, iters=50)
     m = WarmStartMLP(seed=0)
     first = None
     idx = torch.randperm(len(T), device="cuda")
-    for epoch in range(60):
+    for epoch in range(80):
         for k in range(0, len(T), 4096):
             sel = idx[k:k + 4096]
             loss = m.train_step(F[sel], T[sel], lr=2e-3)
@@ -80,6 +83,7 @@ def test_training_lowers_loss_and_warm_start_saves_iterations():
             first = float(loss.item())
     last = float(loss.item())
     assert last < 0.5 * first, (first, last)
-    res = iterations_to_tol(s, m, tol=1e-4, max_iters=50)
-    assert res["learned_with_fallback"] <= res["plain"]
-    assert res["learned"] * 2 <= res["plain"], res
+    res = iterations_to_tol(s, m, tol=1e-4, max_iters=100)
+    assert res["plain"] <= 100, res  # the plain solve converges, slowly
+    assert not res["fallback"], res
+    assert res["learned_with_fallback"] * 2 <= res["plain"], res

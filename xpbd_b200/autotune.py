@@ -71,10 +71,13 @@ def tune6(s, frames=3, candidates=None):
     s._flush()
     key = ("6dof", s.num_bodies, s.cap, s.num_joints, s.substeps, s.iterations, s.broadphase)
     if key in _CACHE and candidates is None:
-        s.set_driver(*_CACHE[key][0])
+        best = _CACHE[key][0]
+        s.lanes = best[3] if len(best) > 3 else 8
+        s.set_driver(*best[:3])
         return _CACHE[key][1]
     if candidates is None:
-        candidates = [(2, 16, 512), (2, 16, 256), (2, 8, 512), (2, 4, 512), (0, 0, 256), (0, 0, 128)]
+        candidates = [(2, 16, 512, 8), (2, 16, 256, 8), (2, 8, 512, 8), (0, 0, 256, 8), (0, 0, 512, 8),
+                      (2, 16, 512, 1), (2, 16, 256, 1), (0, 0, 256, 1)]
     stream = torch.cuda.current_stream(s.device)
     sp = C.c_void_p(stream.cuda_stream)
     L = lib6()
@@ -85,9 +88,11 @@ def tune6(s, frames=3, candidates=None):
     results = {}
     for cand in candidates:
         try:
-            s.set_driver(*cand)
+            lanes = cand[3] if len(cand) > 3 else 8
+            s.lanes = lanes
+            s.set_driver(*cand[:3])
             info = s.launch_info()
-            tag = (info["mode"], info["blocks"], info["threads"])
+            tag = (info["mode"], info["blocks"], info["threads"], lanes)
             if tag in results:
                 continue
             ms = _time(lambda: N.check(L.xpbd6_substeps(s._h, sp)), stream, frames)
@@ -96,8 +101,9 @@ def tune6(s, frames=3, candidates=None):
             s.load_state_dict(snap)
     best_tag = min(results, key=lambda t: results[t][0])
     best = results[best_tag][1]
-    s.set_driver(*best)
-    report = {"chosen": {"mode": best_tag[0], "blocks": best_tag[1], "threads": best_tag[2]},
-              "ms_per_frame": {f"{t[0]}x{t[1]}x{t[2]}": round(v[0], 5) for t, v in results.items()}}
+    s.lanes = best[3] if len(best) > 3 else 8
+    s.set_driver(*best[:3])
+    report = {"chosen": {"mode": best_tag[0], "blocks": best_tag[1], "threads": best_tag[2], "lanes": best_tag[3]},
+              "ms_per_frame": {f"{t[0]}x{t[1]}x{t[2]}x{t[3]}": round(v[0], 5) for t, v in results.items()}}
     _CACHE[key] = (best, report)
     return report

@@ -476,6 +476,403 @@ XD void body_apply_velocity6(const Dev6& s, int i, const Par6& p) {
   s.w[i] = f4(wi, 0.0f);
 }
 
+// =================================================================================
+// Quarter-warp variants: 8 lanes cooperate on one floor body (one lane per box
+// corner), one contact pair (one lane per manifold point) or one manifold
+// generation (one lane per SAT axis, then one lane per polygon vertex through
+// the clip).  Each lane evaluates exactly the per-corner / per-point / per-vertex
+// expressions of the thread-per-item versions above; sums over a body's corners
+// or a pair's points are gathered across the 8 lanes and added in corner / point
+// order, so the result is bit-identical to the thread-per-item loop.
+// This cuts the dependent chain of a phase by up to 8x.
+// =================================================================================
+struct Grp {
+  int l;          // lane within the group (0..7)
+  int base;       // first lane of the group within the warp
+  unsigned mask;  // the group's lanes
+};
+XD Grp grp8() {
+  int lane = threadIdx.x & 31;
+  return Grp{lane & 7, lane & ~7, 0xFFu << (lane & ~7)};
+}
+XD float gsum(const Grp& G, float v) {
+  v += __shfl_xor_sync(G.mask, v, 4);
+  v += __shfl_xor_sync(G.mask, v, 2);
+  v += __shfl_xor_sync(G.mask, v, 1);
+  return v;
+}
+XD V3 gshfl3(const Grp& G, V3 v, int src) {
+  return V3{__shfl_sync(G.mask, v.x, G.base + src), __shfl_sync(G.mask, v.y, G.base + src),
+            __shfl_sync(G.mask, v.z, G.base + src)};
+}
+XD V3 gsum3(const Grp& G, V3 v) { return V3{gsum(G, v.x), gsum(G, v.y), gsum(G, v.z)}; }
+// Sum in lane order, acc = ((0 + t0) + t1) + ... + t7: the association of the
+// thread-per-item loops (and of the reference's per-thread loops), so both
+// phase shapes round identically.  Lanes with no term pass 0 (x + 0 == x).
+// Counts are sums of 1.0 and exact in any order; they use the tree sum above.
+XD V3 gseq3(const Grp& G, V3 v) {
+  V3 acc = V3{0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc = acc + gshfl3(G, v, k);
+  return acc;
+}
+// Two terms per lane, added one after the other: acc = (acc + a_k) + b_k.
+XD V3 gseq3x2(const Grp& G, V3 a, V3 b) {
+  V3 acc = V3{0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    acc = acc + gshfl3(G, a, k);
+    acc = acc + gshfl3(G, b, k);
+  }
+  return acc;
+}
+XD int gscan_ex(const Grp& G, int v, int* total) {  // exclusive prefix within the group
+  int inc = v;
+  for (int o = 1; o < 8; o <<= 1) {
+    int y = __shfl_up_sync(G.mask, inc, o, 8);
+    if (G.l >= o) inc += y;
+  }
+  *total = __shfl_sync(G.mask, inc, G.base + 7);
+  return inc - v;
+}
+
+XD void floor_body8(const Dev6& s, int i, const Par6& p, const Grp& G) {
+  float4 x4 = s.x[i];
+  float im = x4.w;
+  if (im == 0.0f) return;
+  V3 xi = v3(x4), he = v3(s.he[i]), Ii = v3(s.inv_I[i]);
+  Q4 qi = q4(s.q[i]);
+  const V3 S = V3{0.0f, 1.0f, 0.0f};
+  // normal (dx, dr) and friction (fx, fr) terms of this lane's corner
+  V3 dx = V3{0.0f, 0.0f, 0.0f}, dr = V3{0.0f, 0.0f, 0.0f};
+  V3 fx = V3{0.0f, 0.0f, 0.0f}, fr = V3{0.0f, 0.0f, 0.0f};
+  float cnt = 0.0f;
+  const int c = G.l;
+  V3 corner = box_corner(he, c);
+  V3 p1 = xi + qrot(qi, corner);
+  float d = p.floor_y - p1.y;
+  const int slot = 8 * i + c;
+  if (d <= 0.0f) {
+    s.lam_floor[slot] = 0.0f;
+  } else {
+    V3 r = p1 - xi;
+    float wg = gen_inv_mass(im, qi, Ii, r, S);
+    if (wg > 0.0f) {
+      float dlam = d / wg;
+      s.lam_floor[slot] = dlam;
+      V3 P = S * dlam;
+      dx = P * im;
+      dr = world_invI_mul(qi, Ii, cross(r, P));
+      cnt = 1.0f;
+      if (p.mu > 0.0f) {
+        V3 p1b = v3(s.xp[i]) + qrot(q4(s.qp[i]), corner);
+        V3 dp = p1 - p1b;
+        V3 dpt = dp - S * dot(dp, S);
+        float lt = length(dpt);
+        if (lt > kEps && lt < p.mu * d) {
+          float w2 = gen_inv_mass(im, qi, Ii, r, dpt / lt);
+          if (w2 > 0.0f) {
+            V3 pf = (-dpt) / w2;
+            fx = pf * im;
+            fr = world_invI_mul(qi, Ii, cross(r, pf));
+          }
+        }
+      }
+    }
+  }
+  cnt = gsum(G, cnt);
+  dx = gseq3x2(G, dx, fx);
+  dr = gseq3x2(G, dr, fr);
+  if (G.l == 0 && cnt > 0.0f) {
+    vadd(s.ax + i, dx, cnt);
+    vadd(s.ar + i, dr, 0.0f);
+  }
+}
+
+XD void box_pair8(const Dev6& s, int pid, const Grp& G) {
+  int4 hdr = s.m_hdr[pid];
+  const int nc = hdr.x;
+  if (nc == 0) return;
+  const int inc = hdr.y, ref = hdr.z;
+  V3 S = v3(s.m_normal[pid]);
+  float4 xi4 = s.x[inc], xr4 = s.x[ref];
+  V3 xi = v3(xi4), xr = v3(xr4);
+  Q4 qi = q4(s.q[inc]), qr = q4(s.q[ref]);
+  V3 Ii = v3(s.inv_I[inc]), Ir = v3(s.inv_I[ref]);
+  const float imi = xi4.w, imr = xr4.w;
+  V3 dxi = V3{0, 0, 0}, dri = V3{0, 0, 0}, dxr = V3{0, 0, 0}, drr = V3{0, 0, 0};
+  float ci = 0.0f, cr = 0.0f;
+  const int c = G.l;
+  if (c < nc) {
+    int slot = 8 * pid + c;
+    V3 p_inc = xi + qrot(qi, v3(s.m_off_inc[slot]));
+    V3 p_ref = xr + qrot(qr, v3(s.m_off_ref[slot]));
+    float C = dot(p_inc - p_ref, S);
+    if (C >= 0.0f) {
+      s.lam_pair[slot] = 0.0f;
+    } else {
+      float d = -C;
+      V3 r_inc = p_inc - xi, r_ref = p_ref - xr;
+      float w_inc = gen_inv_mass(imi, qi, Ii, r_inc, S);
+      float w_ref = gen_inv_mass(imr, qr, Ir, r_ref, S);
+      float wsum = w_inc + w_ref;
+      if (wsum > 0.0f) {
+        float dlam = d / wsum;
+        s.lam_pair[slot] = s.lam_pair[slot] + dlam;
+        V3 P = S * dlam;
+        if (imi > 0.0f) {
+          dxi = P * imi;
+          dri = world_invI_mul(qi, Ii, cross(r_inc, P));
+          ci = 1.0f;
+        }
+        if (imr > 0.0f) {
+          dxr = (-P) * imr;
+          drr = -world_invI_mul(qr, Ir, cross(r_ref, P));
+          cr = 1.0f;
+        }
+      }
+    }
+  }
+  ci = gsum(G, ci);
+  cr = gsum(G, cr);
+  dxi = gseq3(G, dxi);
+  dri = gseq3(G, dri);
+  dxr = gseq3(G, dxr);
+  drr = gseq3(G, drr);
+  if (G.l == 0) {
+    if (ci > 0.0f) {
+      vadd(s.ax + inc, dxi, ci);
+      vadd(s.ar + inc, dri, 0.0f);
+    }
+    if (cr > 0.0f) {
+      vadd(s.ax + ref, dxr, cr);
+      vadd(s.ar + ref, drr, 0.0f);
+    }
+  }
+}
+
+XD void velocity_floor8(const Dev6& s, int i, const Par6& p, const Grp& G) {
+  float4 x4 = s.x[i];
+  float im = x4.w;
+  if (im == 0.0f) return;
+  const V3 S = V3{0.0f, 1.0f, 0.0f};
+  Q4 qi = q4(s.q[i]);
+  V3 Ii = v3(s.inv_I[i]), he = v3(s.he[i]), vi = v3(s.v[i]), wi = v3(s.w[i]);
+  V3 dv = V3{0, 0, 0}, dw = V3{0, 0, 0};
+  float cnt = 0.0f;
+  const int c = G.l;
+  float lam_n = s.lam_floor[8 * i + c];
+  if (lam_n != 0.0f) {
+    V3 r = qrot(qi, box_corner(he, c));
+    V3 vc = vi + cross(wi, r);
+    V3 impulse = velocity_impulse(vc, S, lam_n, p);
+    if (length(impulse) > kEps) {
+      float wg = gen_inv_mass(im, qi, Ii, r, impulse / length(impulse));
+      if (wg > 0.0f) {
+        V3 P = impulse / wg;
+        dv = P * im;
+        dw = world_invI_mul(qi, Ii, cross(r, P));
+        cnt = 1.0f;
+      }
+    }
+  }
+  cnt = gsum(G, cnt);
+  dv = gseq3(G, dv);
+  dw = gseq3(G, dw);
+  if (G.l == 0 && cnt > 0.0f) {
+    vadd(s.av + i, dv, cnt);
+    vadd(s.aw + i, dw, 0.0f);
+  }
+}
+
+XD void velocity_box8(const Dev6& s, int pid, const Par6& p, const Grp& G) {
+  int4 hdr = s.m_hdr[pid];
+  const int nc = hdr.x;
+  if (nc == 0) return;
+  const int ci = hdr.y, cj = hdr.z;
+  V3 S = v3(s.m_normal[pid]);
+  float4 xi4 = s.x[ci], xj4 = s.x[cj];
+  V3 xi = v3(xi4), xj = v3(xj4);
+  Q4 qi = q4(s.q[ci]), qj = q4(s.q[cj]);
+  V3 Ii = v3(s.inv_I[ci]), Ij = v3(s.inv_I[cj]);
+  V3 vi = v3(s.v[ci]), vj = v3(s.v[cj]), wi = v3(s.w[ci]), wj = v3(s.w[cj]);
+  const float imi = xi4.w, imj = xj4.w;
+  V3 dvi = V3{0, 0, 0}, dwi = V3{0, 0, 0}, dvj = V3{0, 0, 0}, dwj = V3{0, 0, 0};
+  float ni = 0.0f, nj = 0.0f;
+  const int c = G.l;
+  if (c < nc) {
+    int slot = 8 * pid + c;
+    float lam_n = s.lam_pair[slot];
+    if (lam_n != 0.0f) {
+      V3 p_inc = xi + qrot(qi, v3(s.m_off_inc[slot]));
+      V3 p_ref = xj + qrot(qj, v3(s.m_off_ref[slot]));
+      V3 ri = p_inc - xi, rj = p_ref - xj;
+      V3 vrel = (vi + cross(wi, ri)) - (vj + cross(wj, rj));
+      V3 impulse = velocity_impulse(vrel, S, lam_n, p);
+      float li = length(impulse);
+      if (li > kEps) {
+        V3 ndir = impulse / li;
+        float wgi = gen_inv_mass(imi, qi, Ii, ri, ndir);
+        float wgj = gen_inv_mass(imj, qj, Ij, rj, ndir);
+        float wsum = wgi + wgj;
+        if (wsum > 0.0f) {
+          V3 P = impulse / wsum;
+          if (imi > 0.0f) {
+            dvi = P * imi;
+            dwi = world_invI_mul(qi, Ii, cross(ri, P));
+            ni = 1.0f;
+          }
+          if (imj > 0.0f) {
+            dvj = (-P) * imj;
+            dwj = -world_invI_mul(qj, Ij, cross(rj, P));
+            nj = 1.0f;
+          }
+        }
+      }
+    }
+  }
+  ni = gsum(G, ni);
+  nj = gsum(G, nj);
+  dvi = gseq3(G, dvi);
+  dwi = gseq3(G, dwi);
+  dvj = gseq3(G, dvj);
+  dwj = gseq3(G, dwj);
+  if (G.l == 0) {
+    if (ni > 0.0f) {
+      vadd(s.av + ci, dvi, ni);
+      vadd(s.aw + ci, dwi, 0.0f);
+    }
+    if (nj > 0.0f) {
+      vadd(s.av + cj, dvj, nj);
+      vadd(s.aw + cj, dwj, 0.0f);
+    }
+  }
+}
+
+// generate_box_manifold with 8 lanes; `stage` is this group's 8-vertex buffer.
+XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float4* stage) {
+  s.lam_pair[8 * pid + G.l] = 0.0f;
+  int2 pr = s.pairs[pid];
+  const int a = pr.x, b = pr.y;
+  V3 cA = v3(s.x[a]), cB = v3(s.x[b]), eA = v3(s.he[a]), eB = v3(s.he[b]);
+  M33 RA = q2m(q4(s.q[a])), RB = q2m(q4(s.q[b]));
+  V3 cBA = cA - cB;
+  // SAT: lane l < 3 tests A's axis l, lane 3..5 tests B's axis l-3
+  float ov = INFINITY;
+  bool sep = false;
+  if (G.l < 6) {
+    const bool onA = G.l < 3;
+    const int k = onA ? G.l : G.l - 3;
+    V3 L = mcol(onA ? RA : RB, k);
+    ov = comp(onA ? eA : eB, k) + proj_radius(L, onA ? RB : RA, onA ? eB : eA) - fabsf(dot(L, cBA));
+    sep = ov < 0.0f;
+    if (!(ov < 1.0e30f)) ov = INFINITY;  // never selected by the sequential `ov < best` test
+  }
+  if (__any_sync(G.mask, sep)) {
+    if (G.l == 0) s.m_hdr[pid] = make_int4(0, 0, 0, 0);
+    return;
+  }
+  int bi = G.l;  // first minimum in axis order (ties keep the earlier axis)
+  for (int o = 4; o; o >>= 1) {
+    float ov2 = __shfl_xor_sync(G.mask, ov, o);
+    int b2 = __shfl_xor_sync(G.mask, bi, o);
+    if (ov2 < ov || (ov2 == ov && b2 < bi)) {
+      ov = ov2;
+      bi = b2;
+    }
+  }
+  V3 best_axis = V3{0.0f, 1.0f, 0.0f};
+  int ref_is_a = 1, best_k = 0;
+  if (ov < INFINITY) {
+    ref_is_a = bi < 3 ? 1 : 0;
+    best_k = bi % 3;
+    best_axis = mcol(ref_is_a ? RA : RB, best_k);
+  }
+  V3 nBA = best_axis;
+  if (dot(nBA, cBA) < 0.0f) nBA = -nBA;
+  int ref_b, inc_b;
+  V3 c_ref, e_ref, c_inc, e_inc, ref_face_n;
+  M33 R_ref, R_inc;
+  if (ref_is_a) {
+    ref_b = a; inc_b = b; c_ref = cA; R_ref = RA; e_ref = eA; c_inc = cB; R_inc = RB; e_inc = eB;
+    ref_face_n = -nBA;
+  } else {
+    ref_b = b; inc_b = a; c_ref = cB; R_ref = RB; e_ref = eB; c_inc = cA; R_inc = RA; e_inc = eA;
+    ref_face_n = nBA;
+  }
+  const int ref_axis = best_k;
+  V3 ref_face_c = c_ref + ref_face_n * comp(e_ref, ref_axis);
+  int ax1 = (ref_axis + 1) % 3, ax2 = (ref_axis + 2) % 3;
+  V3 u_ref = mcol(R_ref, ax1), v_ref = mcol(R_ref, ax2);
+  float eu = comp(e_ref, ax1), ev = comp(e_ref, ax2);
+  int inc_axis = 0;
+  float inc_sign = 1.0f, best_dot = -1.0e30f;
+  for (int k = 0; k < 3; ++k) {
+    V3 col = mcol(R_inc, k);
+    float dp = -dot(col, ref_face_n);
+    if (dp > best_dot) { best_dot = dp; inc_axis = k; inc_sign = 1.0f; }
+    if (-dp > best_dot) { best_dot = -dp; inc_axis = k; inc_sign = -1.0f; }
+  }
+  V3 inc_n = mcol(R_inc, inc_axis) * inc_sign;
+  V3 inc_face_c = c_inc + inc_n * comp(e_inc, inc_axis);
+  int iax1 = (inc_axis + 1) % 3, iax2 = (inc_axis + 2) % 3;
+  V3 iu = mcol(R_inc, iax1), iv = mcol(R_inc, iax2);
+  float ieu = comp(e_inc, iax1), iev = comp(e_inc, iax2);
+  // lane l holds polygon vertex l
+  V3 v = V3{0.0f, 0.0f, 0.0f};
+  if (G.l == 0) v = (inc_face_c + iu * ieu) + iv * iev;
+  else if (G.l == 1) v = (inc_face_c - iu * ieu) + iv * iev;
+  else if (G.l == 2) v = (inc_face_c - iu * ieu) - iv * iev;
+  else if (G.l == 3) v = (inc_face_c + iu * ieu) - iv * iev;
+  int plen = 4;
+  for (int pi = 0; pi < 4; ++pi) {
+    V3 pp, pn;
+    if (pi == 0) { pp = ref_face_c + u_ref * eu; pn = u_ref; }
+    else if (pi == 1) { pp = ref_face_c - u_ref * eu; pn = -u_ref; }
+    else if (pi == 2) { pp = ref_face_c + v_ref * ev; pn = v_ref; }
+    else { pp = ref_face_c - v_ref * ev; pn = -v_ref; }
+    if (plen == 0) {
+      if (G.l == 0) s.m_hdr[pid] = make_int4(0, 0, 0, 0);
+      return;
+    }
+    const bool live = G.l < plen;
+    V3 bp = gshfl3(G, v, (G.l + 1 < plen) ? G.l + 1 : 0);
+    float da = dot(v - pp, pn), db = dot(bp - pp, pn);
+    const bool ea = live && (da <= 0.0f);
+    const bool ei = live && ((da <= 0.0f) ? (db > 0.0f) : (db <= 0.0f));
+    int total;
+    int pos = gscan_ex(G, (int)ea + (int)ei, &total);
+    __syncwarp(G.mask);
+    if (ea && pos < 8) stage[pos] = f4(v, 0.0f);
+    if (ei) {
+      float t = da / (da - db);
+      int q = pos + (ea ? 1 : 0);
+      if (q < 8) stage[q] = f4(v + (bp - v) * t, 0.0f);
+    }
+    __syncwarp(G.mask);
+    plen = min(total, 8);
+    if (G.l < plen) v = v3(stage[G.l]);
+    __syncwarp(G.mask);
+  }
+  if (plen == 0) {
+    if (G.l == 0) s.m_hdr[pid] = make_int4(0, 0, 0, 0);
+    return;
+  }
+  float d_signed = dot(v - ref_face_c, ref_face_n);
+  const bool keep = G.l < plen && d_signed < margin;
+  int nc;
+  int rank = gscan_ex(G, keep ? 1 : 0, &nc);
+  if (keep) {
+    V3 p_ref = v - ref_face_n * d_signed;
+    s.m_off_inc[8 * pid + rank] = f4(mtv(R_inc, v - c_inc), 0.0f);
+    s.m_off_ref[8 * pid + rank] = f4(mtv(R_ref, p_ref - c_ref), 0.0f);
+  }
+  if (G.l == 0) {
+    s.m_hdr[pid] = make_int4(nc, inc_b, ref_b, 0);
+    s.m_normal[pid] = f4(ref_face_n, 0.0f);
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // Persistent substep kernel: every substep of one frame in one launch.
 __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier bar) {
@@ -525,6 +922,67 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
     }
     grid_sync(bar);
   }
+}
+
+// Persistent substep kernel, quarter-warp phases (manifold, floor, box,
+// velocity): same phase order and barriers as k6_substeps.
+__global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier bar) {
+  __shared__ float4 stage[512 / 8][8];
+  const int n = s.n, nj = s.nj;
+  const int np = min(*s.n_pairs, s.cap);
+  const int t0 = gtid(), st = gstride();
+  const Grp G = grp8();
+  const int g0 = t0 >> 3, gs = st >> 3;
+  float4* my_stage = stage[threadIdx.x >> 3];
+  const int nb = max(n, nj);
+  for (int i = t0; i < nb; i += st) {
+    if (i < n) body_integrate6(s, i, p);
+    if (i < nj) s.lam_joint[i] = 0.0f;
+  }
+  grid_sync(bar);
+  for (int sub = 0; sub < p.substeps; ++sub) {
+    const bool more = sub + 1 < p.substeps;
+    for (int pid = g0; pid < np; pid += gs) manifold_pair8(s, pid, p.margin, G, my_stage);
+    grid_sync(bar);
+    for (int it = 0; it < p.iterations; ++it) {
+      for (int t = t0; t < nj; t += st) joint_row(s, t, p.h);
+      for (int g = g0; g < n + np; g += gs) {
+        if (g < n) floor_body8(s, g, p, G);
+        else box_pair8(s, g - n, G);
+      }
+      grid_sync(bar);
+      const bool last = it + 1 == p.iterations;
+      for (int i = t0; i < n; i += st) {
+        body_apply6(s, i, p.relax);
+        if (last) body_finalize6(s, i, p);
+      }
+      grid_sync(bar);
+    }
+    if (p.iterations == 0) {
+      for (int i = t0; i < n; i += st) body_finalize6(s, i, p);
+      grid_sync(bar);
+    }
+    for (int g = g0; g < n + np; g += gs) {
+      if (g < n) velocity_floor8(s, g, p, G);
+      else velocity_box8(s, g - n, p, G);
+    }
+    grid_sync(bar);
+    for (int i = t0; i < nb; i += st) {
+      if (i < n) {
+        body_apply_velocity6(s, i, p);
+        if (more) body_integrate6(s, i, p);
+      }
+      if (more && i < nj) s.lam_joint[i] = 0.0f;
+    }
+    grid_sync(bar);
+  }
+}
+
+__global__ void k6_manifold8(Dev6 s, float margin) {
+  __shared__ float4 stage[256 / 8][8];
+  const int np = min(*s.n_pairs, s.cap);
+  const Grp G = grp8();
+  for (int pid = gtid() >> 3; pid < np; pid += gstride() >> 3) manifold_pair8(s, pid, margin, G, stage[threadIdx.x >> 3]);
 }
 
 // per-kernel entry points (parity tests)
@@ -1235,6 +1693,7 @@ struct xpbd6_solver {
   unsigned* bar = nullptr;  // count, gen, status
   int blocks = 1, threads = 256, mode = 0;
   int force_mode = -1, force_blocks = 0, force_threads = 0;
+  int lanes = 8;  // 8: quarter-warp phases (k6_substeps8), 1: thread per item (k6_substeps)
   double hg_rsmax = 0.0, hg_cell = 0.0, maxhe = 0.0;
   cudaGraphExec_t graph = nullptr;
 };
@@ -1278,6 +1737,21 @@ extern "C" int xpbd6_set_driver(xpbd6_solver* h, int mode, int blocks, int threa
   return XPBD_OK;
 }
 
+// Phase granularity for the next bind: 8 = quarter-warp per body / pair, 1 = thread per item.
+extern "C" int xpbd6_set_lanes(xpbd6_solver* h, int lanes) {
+  if (!h || (lanes != 1 && lanes != 8)) return XPBD_ERR_BAD_ARG;
+  h->lanes = lanes;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd6_manifold8(const xpbd6_state* s, float margin, void* stream) {
+  if (check6(s)) return XPBD_ERR_BAD_ARG;
+  if (s->pair_capacity == 0) return XPBD_OK;
+  k6_manifold8<<<stream_blocks(8LL * s->pair_capacity, 256), 256, 0, as_stream(stream)>>>(make_dev6(s), margin);
+  XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
 // Host constants of the hash-grid and grid broad phases (solver_6dof.py:335-337, 244).
 extern "C" int xpbd6_set_grid_constants(xpbd6_solver* h, double rs_max, double cell, double max_he) {
   if (!h) return XPBD_ERR_BAD_ARG;
@@ -1287,8 +1761,11 @@ extern "C" int xpbd6_set_grid_constants(xpbd6_solver* h, double rs_max, double c
   return XPBD_OK;
 }
 
-static int cluster_fit6(int want, int threads) {
-  cudaError_t e = cudaFuncSetAttribute(k6_substeps, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+using SubstepKernel = void (*)(Dev6, Par6, GridBarrier);
+static SubstepKernel substep_kernel(const xpbd6_solver* h) { return h->lanes == 8 ? k6_substeps8 : k6_substeps; }
+
+static int cluster_fit6(SubstepKernel kern, int want, int threads) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) {
     set_last_error("cudaFuncSetAttribute", e);
     return -1;
@@ -1305,7 +1782,7 @@ static int cluster_fit6(int want, int threads) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k6_substeps, &cfg) == cudaSuccess && n > 0) return c;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess && n > 0) return c;
     cudaGetLastError();
   }
   return 1;
@@ -1367,7 +1844,7 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
   h->threads = h->force_threads > 0 ? h->force_threads : (mode == 2 ? 512 : 256);
   if (mode == 2) {
     int want = h->force_blocks > 0 ? h->force_blocks : std::max(2, std::min(16, ceil_div(work, h->threads)));
-    int c = cluster_fit6(want, h->threads);
+    int c = cluster_fit6(substep_kernel(h), want, h->threads);
     if (c < 0) return XPBD_ERR_CUDA;
     if (c >= 2) {
       h->mode = 2;
@@ -1378,7 +1855,7 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
   }
   h->mode = 0;
   int per_sm = 0;
-  XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k6_substeps, h->threads, 0));
+  XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, substep_kernel(h), h->threads, 0));
   per_sm = std::max(per_sm, 1);
   int want = std::max(1, ceil_div(work, h->threads));
   h->blocks = std::min(h->force_blocks > 0 ? h->force_blocks : want, per_sm * num_sms());
@@ -1460,7 +1937,7 @@ static int run_substeps(xpbd6_solver* h, cudaStream_t st) {
   }
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  XPBD_CUDA(cudaLaunchKernelEx(&cfg, k6_substeps, h->dev, h->p6, gb));
+  XPBD_CUDA(cudaLaunchKernelEx(&cfg, substep_kernel(h), h->dev, h->p6, gb));
   return XPBD_OK;
 }
 

@@ -69,6 +69,8 @@ _SIGS6 = {
     "xpbd6_step": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
     "xpbd6_status": ([C.c_void_p, C.POINTER(C.c_int), C.c_void_p], C.c_int),
     "xpbd6_set_driver": ([C.c_void_p, C.c_int, C.c_int, C.c_int], C.c_int),
+    "xpbd6_set_lanes": ([C.c_void_p, C.c_int], C.c_int),
+    "xpbd6_manifold8": ([C.c_void_p, C.c_float, C.c_void_p], C.c_int),
     "xpbd6_set_grid_constants": ([C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
     "xpbd6_launch_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "xpbd6_morton": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
@@ -136,6 +138,7 @@ class Solver6DOF:
         self._n_pairs_host = 0
         self.sync_pairs = True
         self.driver = (-1, 0, 0)  # (mode, blocks, threads): -1 automatic; see set_driver
+        self.lanes = 8            # lanes per floor body / contact pair in the substep phases
         self._scene_default = 0
 
     # ---- scene building (solver_6dof.py:166-229) ----------------------------------
@@ -306,7 +309,7 @@ class Solver6DOF:
         """solver_6dof.py:481-487: parameters baked into a bound handle / graph."""
         return (self.cap, self.substeps, self.iterations, self.gyroscopic, self.dt, self.gravity, self.floor_y,
                 self.friction, self.restitution, self.lin_damp, self.ang_damp, self.jacobi_relax, self.max_speed,
-                self.max_omega, self._man_margin, self.broadphase, self.driver)
+                self.max_omega, self._man_margin, self.broadphase, self.driver, self.lanes)
 
     def _bind(self):
         L = lib6()
@@ -317,6 +320,7 @@ class Solver6DOF:
         self._st = self._state()
         self._par = self._params()
         N.check(L.xpbd6_set_driver(self._h, *[int(v) for v in self.driver]), "xpbd6_set_driver")
+        N.check(L.xpbd6_set_lanes(self._h, int(self.lanes)), "xpbd6_set_lanes")
         N.check(L.xpbd6_set_grid_constants(self._h, self._rs_max, self._hg_cell, self._rs_max),
                 "xpbd6_set_grid_constants")
         N.check(L.xpbd6_bind(self._h, C.byref(self._st), C.byref(self._par)), "xpbd6_bind")
