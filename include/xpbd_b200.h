@@ -277,6 +277,20 @@ int xpbd6_set_grid_constants(xpbd6_solver* h, double rs_max, double cell, double
  * NULL = one scene) into out_scene[n_scenes]. */
 int xpbd6_residual(const xpbd6_state* s, const xpbd6_params* p, const int* body_scene, int n_scenes,
                    float* out_scene, void* stream);
+
+/* Learned lambda warm start for the 6-DOF contact rows (network: xpbd_mlp_*
+ * above; no reference counterpart: the reference zeroes these multipliers
+ * every substep, solver_6dof.py:374, kernels_6dof.py:237).  Rows:
+ * [0, 8 n_bodies) floor corner slots (8 i + c), then [8 n_bodies, 8 n_bodies +
+ * 8 pair_capacity) manifold point slots (8 n_bodies + 8 p + c); feats float[rows][8],
+ * weff float[rows].  prev_floor (8 n_bodies) and prev_pair (8 pair_capacity) hold
+ * each slot's multiplier over the previous substep (floor: the total impulse).
+ * Call after xpbd6_integrate and xpbd6_manifold. */
+int xpbd6_features(const xpbd6_state* s, const xpbd6_params* p, const float* prev_floor, const float* prev_pair,
+                   float* feats, float* weff, void* stream);
+/* lambda := lambda0 on every row in contact, with its position / rotation
+ * correction accumulated into the Jacobi sums (apply with xpbd6_apply_jacobi). */
+int xpbd6_warm_start(const xpbd6_state* s, const xpbd6_params* p, const float* lam0, void* stream);
 /* Morton keys of the LBVH over lowers/uppers (float4[n]) -> uint32[n]. */
 int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream);
 

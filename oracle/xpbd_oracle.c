@@ -1297,9 +1297,11 @@ float or6_residual(const or6_scene *S, float floor_y, float h) {
 /* ---------------------------------------------------------------------- */
 /* Learned warm start MLP (no reference counterpart): 7 -> 64 -> 64 -> 1 with
  * GELU, weights rounded to bf16 (round to nearest even), fp32 arithmetic with
- * double-precision sums for the batch reductions.  Mean squared error over the
- * batch (loss = mean e^2) and its gradient d(0.5 mean e^2)/dw, the quantity
- * the engine's training kernel accumulates. */
+ * double-precision sums for the batch reductions.  The prediction is residual
+ * on the previous multiplier: y = x[3] + MLP(x) (x[3] is the transformed
+ * previous-substep multiplier, in the units of the target).  Mean squared
+ * error over the batch (loss = mean e^2, e = y - target) and its gradient
+ * d(0.5 mean e^2)/dw, the quantity the engine's training kernel accumulates. */
 #define MLP_IN 7
 #define MLP_H 64
 #define MLP_NP (MLP_H * MLP_IN + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1)
@@ -1346,6 +1348,7 @@ double or_mlp_grads(const float *feats, const float *targets, int B, const float
         }
         float y = B3[0];
         for (int u = 0; u < MLP_H; ++u) y = fmaf(W3[u], a2[u], y);
+        y = y + x[3];
         double e = (double)y - (double)targets[s];
         loss += e * e;
         double dy = e / (double)B;
@@ -1372,7 +1375,7 @@ double or_mlp_grads(const float *feats, const float *targets, int B, const float
     return loss / (double)B;
 }
 
-/* Forward pass only (predicted y per sample). */
+/* Forward pass only (predicted y = x[3] + MLP(x) per sample). */
 void or_mlp_forward(const float *feats, int B, const float *w_in, float *y_out) {
     float W[MLP_NP];
     for (int i = 0; i < MLP_NP; ++i) W[i] = or_bf16_round(w_in[i]);
@@ -1392,6 +1395,6 @@ void or_mlp_forward(const float *feats, int B, const float *w_in, float *y_out) 
             for (int k = 0; k < MLP_H; ++k) z = fmaf(W2[u * MLP_H + k], a1[k], z);
             y = fmaf(W3[u], or_gelu(z), y);
         }
-        y_out[s] = y;
+        y_out[s] = y + x[3];
     }
 }

@@ -17,45 +17,36 @@
 //   5 cos(normal, gravity)
 //   6 relative normal velocity (v_a - v_b) . n
 // They enter the network through fixed transforms (signed log of lengths in
-// units of 1 mm, log10 of w and alpha~); the network predicts
-//   y = slog(lambda (w + alpha~) / 1 mm)
-// (lambda times the effective stiffness is a length), and lambda0 =
-// slog^-1(y) 1 mm / (w + alpha~).
+// units of 1 mm, log10 of w and alpha~); the prediction is
+//   y = slog(lambda (w + alpha~) / 1 mm) = f3 + MLP(f)
+// (lambda times the effective stiffness is a length; f3 is the same transform
+// of the previous multiplier, so the network learns the change from the
+// previous substep and passing the previous multiplier through costs it
+// nothing), and lambda0 = slog^-1(y) 1 mm / (w + alpha~).  For the 6-DOF
+// contact rows (xpbd6.cu) the same features and the same network are used.
 //
 // Training: `k_mlp_grads` evaluates the mean squared error of a batch and its
 // gradient with respect to every weight, 64 samples per CTA, all activations in
 // shared memory; `k_adam` updates fp32 master weights and their bf16 copy.
 #include <cuda_bf16.h>
 
-#include "engine.cuh"
+#include "learned.cuh"
 
 namespace xpbd {
 
-constexpr int kIn = 7, kHid = 64;
 constexpr int oW1 = 0, oB1 = oW1 + kHid * kIn, oW2 = oB1 + kHid, oB2 = oW2 + kHid * kHid, oW3 = oB2 + kHid,
               oB3 = oW3 + kHid, kNParam = oB3 + 1;  // 4737
-constexpr float kLen = 1.0e-3f;
 
-XD float slog(float x) { return copysignf(log1pf(fabsf(x)), x); }
-XD float slog_inv(float y) { return copysignf(expm1f(fabsf(y)), y); }
 XD float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 XD float gelu_d(float x) {
   return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
 }
 
-struct RowFeat {
-  float f[kIn];
-  float weff;  // w + alpha~ (0: row inactive for the warm start)
-};
-
 // Raw features of row j at the current (predicted) positions.
 XD RowFeat row_features(const float4* x, const float4* v, const int4* ri, const float4* rf, const float4* ra,
                         const float* lam, int j, float h, V3 gdir) {
-  RowFeat o;
-  for (int k = 0; k < kIn; ++k) o.f[k] = 0.0f;
-  o.weff = 0.0f;
   int4 r = ri[j];
-  if (r.w == 0) return o;
+  if (r.w == 0) return no_features();
   float4 f = rf[j];
   float4 xa = x[r.y];
   float wa = xa.w, wb = 0.0f, C = 0.0f, alpha = 0.0f, depth = 0.0f;
@@ -74,33 +65,22 @@ XD RowFeat row_features(const float4* x, const float4* v, const int4* ri, const 
     }
     V3 d = v3(xa) - v3(pb);
     float L = length(d);
-    if (L < kEps) return o;
+    if (L < kEps) return no_features();
     n = d / L;
     C = L - f.x;
     if (r.x == XPBD_CONTACT) depth = C < 0.0f ? -C : 0.0f;
     if (r.x != XPBD_CONTACT) alpha = f.y / (h * h);
   }
   float w = wa + wb;
-  if (w == 0.0f) return o;
-  o.weff = w + alpha;
-  o.f[0] = slog(C / kLen);
-  o.f[1] = log10f(w);
-  o.f[2] = log10f(alpha + 1.0e-12f);
-  o.f[3] = slog(lam[j] * o.weff / kLen);
-  o.f[4] = slog(depth / kLen);
-  o.f[5] = dot(n, gdir);
-  o.f[6] = slog(dot(vrel, n) * h / kLen);
-  return o;
+  if (w == 0.0f) return no_features();
+  return pack_features(C, w, alpha, lam[j], depth, dot(n, gdir), dot(vrel, n), h);
 }
 
 __global__ void k3_features(const float4* x, const float4* v, const int4* ri, const float4* rf, const float4* ra,
                             const float* lam, const int* n_rows, float h, V3 gdir, float* feats, float* weff) {
   const int m = *n_rows;
   for (int j = gtid(); j < m; j += gstride()) {
-    RowFeat o = row_features(x, v, ri, rf, ra, lam, j, h, gdir);
-    for (int k = 0; k < kIn; ++k) feats[(size_t)j * 8 + k] = o.f[k];
-    feats[(size_t)j * 8 + 7] = 0.0f;
-    weff[j] = o.weff;
+    store_features(row_features(x, v, ri, rf, ra, lam, j, h, gdir), feats, weff, (size_t)j);
   }
 }
 
@@ -130,7 +110,7 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const float* feats, const flo
       for (int k = 0; k < kHid; ++k) z = __fmaf_rn(W[oW2 + u * kHid + k], a1[k], z);
       y = __fmaf_rn(W[oW3 + u], gelu(z), y);
     }
-    lam0[j] = slog_inv(y) * kLen / we;
+    lam0[j] = slog_inv(y + in[3]) * kLen / we;
   }
 }
 
@@ -182,7 +162,7 @@ __global__ void __launch_bounds__(256) k_mlp_grads(const float* feats, const flo
     for (int s = t; s < kTile; s += T) {  // output + loss
       float y = W[oB3];
       for (int u = 0; u < kHid; ++u) y = __fmaf_rn(W[oW3 + u], gelu(Z2[s * kHid + u]), y);
-      float e = s < ns ? y - targets[base + s] : 0.0f;
+      float e = s < ns ? (y + X[s * 8 + 3]) - targets[base + s] : 0.0f;
       lsum += e * e;
       DY[s] = e / (float)B;  // d(mean 0.5 e^2)/dy... scaled below
     }

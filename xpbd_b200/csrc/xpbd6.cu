@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "learned.cuh"
 #include "prims.cuh"
 
 namespace xpbd {
@@ -1569,6 +1570,104 @@ __global__ void k6_grid_write(Dev6 s, BP6 b, double man_margin, double dt, doubl
 // =================================================================================
 using namespace xpbd;
 
+// =================================================================================
+// Learned lambda warm start for the contact rows (no reference counterpart; the
+// reference restarts every substep from lambda = 0, solver_6dof.py:374 and
+// kernels_6dof.py:237).  Row layout of the feature / lambda0 arrays:
+//   [0, 8n)             floor corner slots, body i corner c -> 8 i + c
+//   [8n, 8n + 8 cap)    manifold point slots, pair p point c -> 8n + 8 p + c
+// Both row kinds are one-sided (lambda >= 0 pushes C < 0 back towards 0).  The
+// floor slots' multiplier is assigned, not accumulated, by the reference's floor
+// solve (kernels_6dof.py:193), so their "lambda" here is the total impulse of a
+// substep (the sum of its iterations' assignments), kept by the caller.
+// =================================================================================
+XD RowFeat floor_row_features(const Dev6& s, int slot, const Par6& p, const float* lam_prev, V3 gdir) {
+  const int i = slot >> 3, c = slot & 7;
+  const float4 x4 = s.x[i];
+  if (x4.w == 0.0f) return no_features();
+  const Q4 qi = q4(s.q[i]);
+  const V3 r = qrot(qi, box_corner(v3(s.he[i]), c));
+  const V3 S = V3{0.0f, 1.0f, 0.0f};
+  const float w = gen_inv_mass(x4.w, qi, v3(s.inv_I[i]), r, S);
+  if (!(w > 0.0f)) return no_features();
+  const float C = (x4.y + r.y) - p.floor_y;
+  const float vn = dot(v3(s.v[i]) + cross(v3(s.w[i]), r), S);
+  return pack_features(C, w, 0.0f, lam_prev[slot], C < 0.0f ? -C : 0.0f, dot(S, gdir), vn, p.h);
+}
+
+XD RowFeat pair_row_features(const Dev6& s, int slot, const Par6& p, const float* lam_prev, V3 gdir) {
+  const int pid = slot >> 3, c = slot & 7;
+  if (pid >= min(*s.n_pairs, s.cap)) return no_features();
+  const int4 hdr = s.m_hdr[pid];
+  if (c >= hdr.x) return no_features();
+  const int inc = hdr.y, ref = hdr.z;
+  const V3 S = v3(s.m_normal[pid]);
+  const float4 xi4 = s.x[inc], xr4 = s.x[ref];
+  const Q4 qi = q4(s.q[inc]), qr = q4(s.q[ref]);
+  const V3 ri = qrot(qi, v3(s.m_off_inc[slot])), rr = qrot(qr, v3(s.m_off_ref[slot]));
+  const float C = dot((v3(xi4) + ri) - (v3(xr4) + rr), S);
+  const float w = gen_inv_mass(xi4.w, qi, v3(s.inv_I[inc]), ri, S) + gen_inv_mass(xr4.w, qr, v3(s.inv_I[ref]), rr, S);
+  if (!(w > 0.0f)) return no_features();
+  const V3 vrel = (v3(s.v[inc]) + cross(v3(s.w[inc]), ri)) - (v3(s.v[ref]) + cross(v3(s.w[ref]), rr));
+  return pack_features(C, w, 0.0f, lam_prev[slot], C < 0.0f ? -C : 0.0f, dot(S, gdir), dot(vrel, S), p.h);
+}
+
+__global__ void k6_features(Dev6 s, Par6 p, const float* prev_floor, const float* prev_pair, V3 gdir, float* feats,
+                            float* weff) {
+  const int nf = 8 * s.n, m = nf + 8 * s.cap;
+  for (int j = gtid(); j < m; j += gstride()) {
+    RowFeat o = j < nf ? floor_row_features(s, j, p, prev_floor, gdir)
+                       : pair_row_features(s, j - nf, p, prev_pair, gdir);
+    store_features(o, feats, weff, (size_t)j);
+  }
+}
+
+// lambda := lambda0 on every row in contact at the predicted positions, and the
+// row's correction M^-1 grad C^T lambda0 (position and rotation) accumulated
+// with count 1 into the Jacobi accumulators, exactly as one floor / manifold
+// solve would; the caller's averaged apply turns the sums into the step.
+__global__ void k6_warm(Dev6 s, Par6 p, const float* lam0) {
+  const int nf = 8 * s.n, m = nf + 8 * s.cap;
+  const int np = min(*s.n_pairs, s.cap);
+  for (int j = gtid(); j < m; j += gstride()) {
+    const float l0 = lam0[j];
+    if (!(l0 > 0.0f) || !isfinite(l0)) continue;
+    if (j < nf) {
+      const int i = j >> 3, c = j & 7;
+      const float4 x4 = s.x[i];
+      if (x4.w == 0.0f) continue;
+      const Q4 qi = q4(s.q[i]);
+      const V3 r = qrot(qi, box_corner(v3(s.he[i]), c));
+      if (!((x4.y + r.y) - p.floor_y < 0.0f)) continue;
+      s.lam_floor[j] = l0;
+      const V3 P = V3{0.0f, l0, 0.0f};
+      vadd(s.ax + i, P * x4.w, 1.0f);
+      vadd(s.ar + i, world_invI_mul(qi, v3(s.inv_I[i]), cross(r, P)), 0.0f);
+    } else {
+      const int slot = j - nf, pid = slot >> 3, c = slot & 7;
+      if (pid >= np) continue;
+      const int4 hdr = s.m_hdr[pid];
+      if (c >= hdr.x) continue;
+      const int inc = hdr.y, ref = hdr.z;
+      const V3 S = v3(s.m_normal[pid]);
+      const float4 xi4 = s.x[inc], xr4 = s.x[ref];
+      const Q4 qi = q4(s.q[inc]), qr = q4(s.q[ref]);
+      const V3 ri = qrot(qi, v3(s.m_off_inc[slot])), rr = qrot(qr, v3(s.m_off_ref[slot]));
+      if (!(dot((v3(xi4) + ri) - (v3(xr4) + rr), S) < 0.0f)) continue;
+      s.lam_pair[slot] = l0;
+      const V3 P = S * l0;
+      if (xi4.w > 0.0f) {
+        vadd(s.ax + inc, P * xi4.w, 1.0f);
+        vadd(s.ar + inc, world_invI_mul(qi, v3(s.inv_I[inc]), cross(ri, P)), 0.0f);
+      }
+      if (xr4.w > 0.0f) {
+        vadd(s.ax + ref, (-P) * xr4.w, 1.0f);
+        vadd(s.ar + ref, -world_invI_mul(qr, v3(s.inv_I[ref]), cross(rr, P)), 0.0f);
+      }
+    }
+  }
+}
+
 static Dev6 make_dev6(const xpbd6_state* s) {
   Dev6 d;
   d.x = reinterpret_cast<float4*>(s->x);
@@ -1667,6 +1766,22 @@ extern "C" int xpbd6_solve_velocities(const xpbd6_state* s, const xpbd6_params* 
 }
 extern "C" int xpbd6_apply_velocity(const xpbd6_state* s, const xpbd6_params* p, void* stream) {
   XPBD6_LAUNCH(k6_apply_velocity, s->n_bodies, make_dev6(s), make_par6(p));
+}
+
+static V3 gravity_dir(const xpbd6_params* p) {
+  const float* g = p->gravity;
+  float gl = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  return gl > 0.0f ? V3{g[0] / gl, g[1] / gl, g[2] / gl} : V3{0.0f, -1.0f, 0.0f};
+}
+extern "C" int xpbd6_features(const xpbd6_state* s, const xpbd6_params* p, const float* prev_floor,
+                              const float* prev_pair, float* feats, float* weff, void* stream) {
+  if (!prev_floor || !prev_pair || !feats || !weff) return XPBD_ERR_BAD_ARG;
+  XPBD6_LAUNCH(k6_features, 8LL * ((long long)s->n_bodies + s->pair_capacity), make_dev6(s), make_par6(p),
+               prev_floor, prev_pair, gravity_dir(p), feats, weff);
+}
+extern "C" int xpbd6_warm_start(const xpbd6_state* s, const xpbd6_params* p, const float* lam0, void* stream) {
+  if (!lam0) return XPBD_ERR_BAD_ARG;
+  XPBD6_LAUNCH(k6_warm, 8LL * ((long long)s->n_bodies + s->pair_capacity), make_dev6(s), make_par6(p), lam0);
 }
 
 __global__ void k6_body_aabb(Dev6 s, Par6 p, float4* lo, float4* hi) {

@@ -1,10 +1,12 @@
-"""Learned lambda warm start for the 3-DOF solver (no reference counterpart).
+"""Learned lambda warm start for the 3-DOF rows and the 6-DOF contact rows (no
+reference counterpart).
 
 The reference restarts every substep from lambda = 0 (solver.py:430-431).  Here a
 small MLP (7 -> 64 -> 64 -> 1, GELU, bf16 weights, fp32 accumulation), trained
 by the engine's own kernels on (row features -> multiplier after 50 plain
 iterations) pairs that the plain solver generates, predicts each row's
-multiplier at the start of a substep.  The substep then starts from that
+multiplier at the start of a substep.  The prediction is residual on the
+previous substep's multiplier (in the transformed units: y = f3 + MLP(f)).  The substep then starts from that
 lambda0, with positions pre-corrected by the Jacobi-averaged M^-1 grad C^T
 lambda0, instead of from lambda = 0.
 
@@ -18,6 +20,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 
 import numpy as np
 import torch
@@ -26,6 +29,7 @@ from . import _native as N
 
 N_PARAM = 7 * 64 + 64 + 64 * 64 + 64 + 64 + 1
 LEN = 1.0e-3  # length unit of the feature / target transforms (1 mm)
+PRETRAINED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "warm_start_weights.npy")
 
 
 def _fn(name, args, res=C.c_int):
@@ -99,6 +103,24 @@ class WarmStartMLP:
         N.check(self.F["infer"](N.ptr(feats), N.ptr(weff), int(m), N.ptr(self.wb), N.ptr(lam0),
                                 N.stream_of(self.device)), "xpbd_mlp_infer")
 
+    @classmethod
+    def pretrained(cls, device="cuda:0"):
+        """The shipped network: trained by ``train_warm_start`` on 10M rows from
+        randomized cloths and box piles (``warm_start_weights.npy``)."""
+        m = cls(device=device)
+        m.load_weights(PRETRAINED)
+        return m
+
+    def save_weights(self, path):
+        """fp32 master weights as a flat .npy (4737 values)."""
+        np.save(path, self.w.cpu().numpy())
+
+    def load_weights(self, path):
+        w = np.load(path).astype(np.float32).reshape(-1)
+        if w.size != N_PARAM:
+            raise ValueError(f"{path}: {w.size} weights, expected {N_PARAM}")
+        self.load_state_dict({"w": torch.from_numpy(w)})
+
     def state_dict(self):
         return {"w": self.w.cpu(), "step": self.step_count}
 
@@ -144,9 +166,14 @@ class SubstepKit:
         N.check(self.F["jacobi"](self.st, float(self.h), 1 if first else 0, self.stream()))
         N.check(self.F["apply"](self.st, float(self.s.jacobi_relax), self.stream()))
 
-    def warm(self, model):
+    def warm(self, model=None, lam0=None):
+        """lambda := lambda0 (the network's prediction, or the given per-row
+        lambda0) with its Jacobi-averaged correction applied."""
         m = self.s._cap
-        model.infer(self.feats, self.weff, m, self.lam0)
+        if lam0 is None:
+            model.infer(self.feats, self.weff, m, self.lam0)
+        else:
+            self.lam0.copy_(lam0)
         N.check(self.F["warm"](self.st, N.ptr(self.lam0), self.stream()))
         N.check(self.F["apply"](self.st, float(self.s.jacobi_relax), self.stream()))
 
@@ -186,35 +213,63 @@ def collect(s, substeps, iters=50, every=1):
     return torch.cat(F), torch.cat(T)
 
 
-def iterations_to_tol(s, model=None, tol=1e-4, max_iters=50):
+def iterations_to_tol(s, model=None, tol=1e-4, max_iters=50, advance=False, carry_iters=50, classic=False):
     """From the current state, one substep: the number of Jacobi iterations the
     plain solve (lambda0 = 0) and the warm-started solve need to bring the
-    residual below `tol` (max_iters + 1 if never), with the per-substep fallback
-    to plain when the learned first iteration is worse.  The state is restored."""
+    residual below `tol` (max_iters + 1 if never) and to reach the plain solve's
+    final residual, with the per-substep fallback to plain when the learned
+    first iteration is worse.  The state's multipliers are the previous
+    multipliers of the features.  Without `advance` the state is restored; with
+    it the scene completes the substep with its normal iterations and the plain
+    solve's multipliers after `carry_iters` iterations become the next
+    substep's previous multipliers (the protocol ``collect`` trains on).  With
+    `classic` the warm start from the previous multipliers themselves
+    (lambda0 = lambda_prev) is measured as well."""
     kit = SubstepKit(s)
     snap = s.state_dict()
     out = {}
+    lam_plain = None
 
-    def run(use_model):
+    def first_below(res, t):
+        hit = [i + 1 for i, r in enumerate(res) if r < t]
+        return hit[0] if hit else max_iters + 1
+
+    def run(use_model, lam0=None):
+        nonlocal lam_plain
         s.load_state_dict(snap)
         kit.integrate()
-        if use_model:
+        warm = use_model or lam0 is not None
+        if warm:
             kit.features()
-            kit.warm(model)
+            kit.warm(model, lam0)
         res = []
         for it in range(max_iters):
-            kit.iterate(first=(it == 0 and not use_model))
+            kit.iterate(first=(it == 0 and not warm))
             res.append(kit.residual())
+            if not warm and it + 1 == min(carry_iters, max_iters):
+                lam_plain = s.tensors["lam"].clone()
         s.load_state_dict(snap)
-        hit = [i + 1 for i, r in enumerate(res) if r < tol]
-        return (hit[0] if hit else max_iters + 1), res
+        return first_below(res, tol), res
 
     out["plain"], rp = run(False)
+    out["residual_plain"] = rp
     if model is not None:
         out["learned"], rl = run(True)
         out["fallback"] = rl[0] > rp[0]
         out["learned_with_fallback"] = out["plain"] if out["fallback"] else out["learned"]
         out["residual_first_iter"] = {"plain": rp[0], "learned": rl[0]}
+        out["residual_learned"] = rl
+        out["to_plain_final"] = {"plain": first_below(rp, rp[-1] * (1 + 1e-6)),
+                                 "learned": first_below(rl, rp[-1] * (1 + 1e-6))}
+    if classic:
+        out["classic"], rc = run(False, snap["lam"])
+        out["residual_first_iter"]["classic"] = rc[0]
+    if advance:
+        kit.integrate()
+        for it in range(s.iterations):
+            kit.iterate(first=(it == 0))
+        kit.finalize()
+        s.tensors["lam"].copy_(lam_plain)
     return out
 
 
@@ -292,3 +347,260 @@ class WarmStartRunner:
             with torch.cuda.graph(self.graph):
                 self._frame()
         self.graph.replay()
+
+
+# ---- 6-DOF contact rows ---------------------------------------------------------------
+def _sigs6():
+    from .solver_6dof import lib6
+    L = lib6()
+    for name, args in (("xpbd6_features", [_p, _p, _p, _p, _p, _p, _p]), ("xpbd6_warm_start", [_p, _p, _p, _p])):
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    return L
+
+
+class SubstepKit6:
+    """Per-kernel driving of one ``Solver6DOF`` substep (integrate, manifold,
+    features, warm start, Jacobi iterations, residual, finalize, velocity pass),
+    used for data generation and evaluation of the contact-row warm start.
+
+    Rows: the 8 n floor corner slots, then the 8 cap manifold point slots.  The
+    reference's floor solve assigns (not accumulates) a corner's multiplier each
+    iteration, so the kit keeps each floor slot's total impulse over the substep
+    (``tot_floor``); that total is the floor rows' lambda for features and
+    targets.  Run with ``plain_iterations`` iterations per substep the kit steps
+    the same physics as the persistent substep kernel."""
+
+    def __init__(self, s):
+        s._flush()
+        if s._sig != s._signature():
+            s._bind()
+        self.s = s
+        self.L = _sigs6()
+        self._alloc()
+        self.h = s.dt / s.substeps
+        self._carry = None
+        self._pair_prev = None
+
+    def _alloc(self):
+        s, dev = self.s, self.s.device
+        self.n = s.num_bodies
+        self.cap = s.cap
+        self.nf = 8 * self.n
+        self.rows = 8 * (self.n + self.cap)
+        self.feats = torch.zeros((self.rows, 8), dtype=torch.float32, device=dev)
+        self.weff = torch.zeros(self.rows, dtype=torch.float32, device=dev)
+        self.lam0 = torch.zeros(self.rows, dtype=torch.float32, device=dev)
+        self.prev_floor = torch.zeros(self.nf, dtype=torch.float32, device=dev)
+        self.prev_pair = torch.zeros(8 * self.cap, dtype=torch.float32, device=dev)
+        self.tot_floor = torch.zeros(self.nf, dtype=torch.float32, device=dev)
+
+    @property
+    def st(self):
+        return C.byref(self.s._st)
+
+    @property
+    def par(self):
+        return C.byref(self.s._par)
+
+    def stream(self):
+        return N.stream_of(self.s.device)
+
+    def broadphase(self):
+        """The frame's pair list (grows the pair capacity like ``step``).  The
+        pair slots' previous multipliers follow their pair into the new list
+        (pairs are matched by their (a, b) key); new pairs start at 0."""
+        s, T = self.s, self.s.tensors
+        n_old = min(s.n_pairs, self.cap)
+        old_keys = T["pairs"][:n_old].long()
+        old_keys = old_keys[:, 0] * self.n + old_keys[:, 1]
+        src = self._carry[self.nf:] if self._carry is not None else T["lam_pair"][: 8 * self.cap]
+        old_lam = src.view(-1, 8)[:n_old].clone()
+        old_keys, order = torch.sort(old_keys)  # the host grid emits in grid order
+        old_lam = old_lam[order]
+        N.check(self.L.xpbd6_broadphase(s._h, self.stream()), "xpbd6_broadphase")
+        cnt = s.n_pairs
+        if cnt > s.cap:
+            s._alloc_pairs(int(cnt * 1.5))
+            s._bind()
+            handled = C.c_int(0)
+            N.check(self.L.xpbd6_status(s._h, C.byref(handled), self.stream()), "xpbd6_status")
+            N.check(self.L.xpbd6_broadphase(s._h, self.stream()), "xpbd6_broadphase")
+            prev_floor = self._carry[: self.nf].clone() if self._carry is not None else self.prev_floor.clone()
+            self._alloc()
+            self._carry = None
+            self.prev_floor.copy_(prev_floor)
+        T = s.tensors
+        n_new = min(s.n_pairs, self.cap)
+        keys = T["pairs"][:n_new].long()
+        keys = keys[:, 0] * self.n + keys[:, 1]
+        mapped = torch.zeros((self.cap, 8), dtype=torch.float32, device=s.device)
+        if n_old and n_new:
+            idx = torch.searchsorted(old_keys, keys).clamp_(max=n_old - 1)
+            hit = old_keys[idx] == keys
+            mapped[:n_new][hit] = old_lam[idx[hit]]
+        self._pair_prev = mapped.view(-1)
+
+    def carry(self, lam_rows):
+        """Use these per-row multipliers (for example a converged solve's) as the
+        next substep's previous multipliers."""
+        self._carry = lam_rows.clone()
+
+    def begin(self):
+        """integrate + manifold + features of the next substep."""
+        T = self.s.tensors
+        if self._carry is not None:
+            self.prev_floor.copy_(self._carry[: self.nf])
+            self.prev_pair.copy_(self._carry[self.nf:])
+            self._carry = None
+        else:
+            self.prev_pair.copy_(T["lam_pair"][: 8 * self.cap])
+        if self._pair_prev is not None:  # first substep on a new pair list
+            self.prev_pair.copy_(self._pair_prev)
+            self._pair_prev = None
+        N.check(self.L.xpbd6_integrate(self.st, self.par, self.stream()), "xpbd6_integrate")
+        N.check(self.L.xpbd6_manifold(self.st, float(self.s._man_margin), self.stream()), "xpbd6_manifold")
+        N.check(self.L.xpbd6_features(self.st, self.par, N.ptr(self.prev_floor), N.ptr(self.prev_pair),
+                                      N.ptr(self.feats), N.ptr(self.weff), self.stream()), "xpbd6_features")
+        self.tot_floor.zero_()
+
+    def iterate(self):
+        T = self.s.tensors
+        N.check(self.L.xpbd6_solve_positions(self.st, self.par, 0, self.stream()), "xpbd6_solve_positions")
+        self.tot_floor += T["lam_floor"][: self.nf]
+        N.check(self.L.xpbd6_apply_jacobi(self.st, float(self.s.jacobi_relax), self.stream()), "xpbd6_apply_jacobi")
+
+    def warm(self, model=None, scale=1.0, lam0=None):
+        """lambda := scale * lambda0 (the network's prediction, or the given
+        per-row lambda0) on the rows in contact, with its correction applied."""
+        T = self.s.tensors
+        if lam0 is None:
+            model.infer(self.feats, self.weff, self.rows, self.lam0)
+        else:
+            self.lam0.copy_(lam0)
+        if scale != 1.0:
+            self.lam0.mul_(scale)
+        N.check(self.L.xpbd6_warm_start(self.st, self.par, N.ptr(self.lam0), self.stream()), "xpbd6_warm_start")
+        self.tot_floor += T["lam_floor"][: self.nf]
+        N.check(self.L.xpbd6_apply_jacobi(self.st, float(self.s.jacobi_relax), self.stream()), "xpbd6_apply_jacobi")
+
+    def finish(self):
+        """finalize + velocity pass; the substep's floor totals become the next
+        substep's previous multipliers."""
+        for name in ("xpbd6_finalize", "xpbd6_solve_velocities", "xpbd6_apply_velocity"):
+            N.check(getattr(self.L, name)(self.st, self.par, self.stream()), name)
+        self.prev_floor.copy_(self.tot_floor)
+
+    def snapshot(self):
+        T = self.s.tensors
+        return T["x"].clone(), T["q"].clone()
+
+    def restore(self, snap):
+        """Back to the state right after ``begin`` (multipliers zero)."""
+        T = self.s.tensors
+        T["x"].copy_(snap[0])
+        T["q"].copy_(snap[1])
+        T["lam_floor"].zero_()
+        T["lam_pair"].zero_()
+        self.tot_floor.zero_()
+
+    def residual(self):
+        return float(self.s.residual()[0])
+
+    def lam_rows(self):
+        """Every row's multiplier: floor totals, then the manifold points'."""
+        return torch.cat([self.tot_floor, self.s.tensors["lam_pair"][: 8 * self.cap]])
+
+    def targets_from(self, lam):
+        return torch.sign(lam * self.weff) * torch.log1p(torch.abs(lam * self.weff) / LEN)
+
+    def substep(self, iterations=None):
+        self.begin()
+        for _ in range(self.s.iterations if iterations is None else iterations):
+            self.iterate()
+        self.finish()
+
+
+def collect6(s, frames, iters=50, floor_gap=0.01):
+    """(features, target) pairs from the plain solver on a box scene: the scene
+    advances with its normal iteration count; at every substep the target is
+    the multiplier after `iters` plain iterations from the same post-integrate
+    state, and that multiplier is the next substep's previous multiplier
+    (feature 3).  Floor slots are kept when the corner is within
+    `floor_gap` of the floor or its target is non-zero."""
+    kit = SubstepKit6(s)
+    F, T = [], []
+    gap = float(np.log1p(floor_gap / LEN))
+    for _ in range(frames):
+        kit.broadphase()
+        for _ in range(s.substeps):
+            kit.begin()
+            snap = kit.snapshot()
+            for _ in range(iters):
+                kit.iterate()
+            lam = kit.lam_rows()
+            tgt = kit.targets_from(lam)
+            kit.carry(lam)
+            keep = kit.weff > 0
+            keep[: kit.nf] &= (kit.feats[: kit.nf, 0] < gap) | (tgt[: kit.nf] != 0)
+            F.append(kit.feats[keep].clone())
+            T.append(tgt[keep].clone())
+            kit.restore(snap)
+            for _ in range(s.iterations):
+                kit.iterate()
+            kit.finish()
+    return torch.cat(F), torch.cat(T)
+
+
+def iterations_to_tol6(kit, model=None, tol=1e-4, max_iters=50, scale=1.0, variants=None):
+    """One substep of a box scene from its current state: the residual after
+    every Jacobi iteration of the plain solve (lambda0 = 0) and of the
+    warm-started solve, the iterations each needs to reach `tol` (max_iters + 1
+    if never) and to reach the plain solve's final residual, and the
+    per-substep fallback (plain kept when the learned first iteration is worse).
+    The scene then completes the substep with its normal iterations, and the
+    plain solve's `max_iters`-iteration multipliers become the next substep's
+    previous multipliers (as in ``collect6``)."""
+    s = kit.s
+    kit.begin()
+    snap = kit.snapshot()
+
+    def run(use_model, sc=scale, lam0=None):
+        kit.restore(snap)
+        if use_model or lam0 is not None:
+            kit.warm(model, sc, lam0)
+        res = []
+        for _ in range(max_iters):
+            kit.iterate()
+            res.append(kit.residual())
+        return res
+
+    def first_below(res, t):
+        hit = [i + 1 for i, r in enumerate(res) if r < t]
+        return hit[0] if hit else max_iters + 1
+
+    out = {}
+    rp = run(False)
+    lam_plain = kit.lam_rows().clone()
+    out["plain"] = first_below(rp, tol)
+    out["residual_plain"] = rp
+    if model is not None:
+        rl = run(True)
+        out["learned"] = first_below(rl, tol)
+        out["fallback"] = rl[0] > rp[0]
+        out["learned_with_fallback"] = out["plain"] if out["fallback"] else out["learned"]
+        target = rp[-1]
+        out["to_plain_final"] = {"plain": first_below(rp, target * (1 + 1e-6)),
+                                 "learned": first_below(rl, target * (1 + 1e-6))}
+        out["residual_learned"] = rl
+    for name, (sc, lam0_fn) in (variants or {}).items():
+        rv = run(lam0_fn is None, sc, None if lam0_fn is None else lam0_fn(kit))
+        out[name] = {"first": rv[0], "second": rv[1], "to_tol": first_below(rv, tol),
+                     "to_plain_final": first_below(rv, rp[-1] * (1 + 1e-6)), "final": rv[-1]}
+    kit.restore(snap)
+    for _ in range(s.iterations):
+        kit.iterate()
+    kit.finish()
+    kit.carry(lam_plain)
+    return out

@@ -1,36 +1,49 @@
-"""Train and evaluate the learned lambda warm start (3-DOF cloth) on the GPU.
+"""Train and evaluate the learned lambda warm start on the GPU.
 
-    python -m xpbd_b200.train_warm_start --samples 10000000 --out model.pt
-    python -m xpbd_b200.train_warm_start --eval model.pt
+    python -m xpbd_b200.train_warm_start --samples 10000000 --out weights.npy
+    python -m xpbd_b200.train_warm_start --eval weights.npy
 
-Data: randomized cloths (n x n, n ~ U{32..128}; spacing 0.02 m, 0.01 kg, two
-pinned corners, FLOOR rows at y = 0; compliance log-uniform in [1e-10, 1e-4]),
-each run for a random number of frames with the normal solver, then sampled
-substep by substep: features at the substep start, target = the multiplier
-after 50 plain Jacobi iterations (``learned.collect``).  Training: Adam on the
-mean squared error, by the engine's own gradient and Adam kernels.
+Data (half from each family, by sample count):
+  * randomized cloths (n x n, n ~ U{32..128}; spacing 0.02 m, 0.01 kg, two
+    pinned corners, FLOOR rows at y = 0; compliance log-uniform in
+    [1e-10, 1e-4]), each run for a random number of frames, then sampled substep
+    by substep: features at the substep start, target = the multiplier after 50
+    plain Jacobi iterations (``learned.collect``);
+  * randomized box piles (256..1440 boxes on a near-cubic 0.8 m lattice, half
+    extents U[0.1, 0.3] m, random orientations, mu 0.6, e 0.2), run for a
+    random number of frames, then sampled substep by substep in the same way on
+    the floor-corner and manifold-point rows (``learned.collect6``).
+In both, the previous substep's converged multiplier is feature 3.  Training:
+Adam on the mean squared error, by the engine's own gradient and Adam kernels,
+cosine learning-rate decay.
 
-Evaluation (``evaluate``): a 128 x 128 cloth of the same family at compliance
-1e-5 (where the plain Jacobi solve reaches the tolerance; at compliance <= 1e-6
-it does not within any practical iteration count, from any start), after it
-has been hanging for a while: per sampled substep, the Jacobi iterations the
-plain solve (lambda0 = 0) and the warm-started solve need to bring the residual
-(hard rows max(0, -C), compliant rows |C + alpha~ lambda|) below 1e-4 m, with
-the per-substep fallback to plain when the learned first iteration is worse.
+Evaluation (``evaluate_cloth``, ``evaluate_pile``): per sampled substep, the
+Jacobi iterations the plain solve (lambda0 = 0) and the warm-started solve need
+to bring the max residual (hard rows max(0, -C), compliant rows |C + alpha~
+lambda|) below 1e-4 m, with the per-substep fallback to plain when the learned
+first iteration is worse.  On the 128 x 128 cloth at compliance 1e-5 the plain
+solve reaches 1e-4 m; on the settled 1440-box pile it does not within 50
+iterations (averaged Jacobi through a 10-box-high stack converges slowly), so
+the pile also reports the iterations each start needs to reach the plain
+solve's own 50-iteration residual, and the residual after the configured two.
 """
 
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import time
 
 import numpy as np
 import torch
 
 from . import scenes
-from .learned import WarmStartMLP, collect, iterations_to_tol
+from .learned import SubstepKit6, WarmStartMLP, collect, collect6, iterations_to_tol, iterations_to_tol6
 from .solver import Solver
+from .solver_6dof import Solver6DOF
+
+PILE_KW = dict(dt=1 / 60, substeps=15, iterations=2, floor_y=0.0, friction=0.6, restitution=0.2, broadphase="lbvh")
 
 
 def make_cloth(n, compliance, floor=True):
@@ -39,81 +52,213 @@ def make_cloth(n, compliance, floor=True):
     return s
 
 
-def generate(n_samples, seed=0, substeps_per_cloth=8, log=print):
+def make_pile(k, seed):
+    """About k boxes on a near-cubic 0.8 m lattice (config-2 distributions)."""
+    nx = max(2, int(round((k / 1.2) ** (1 / 3) * 1.1)))
+    ny = max(1, k // (nx * nx))
+    s = Solver6DOF(device="cuda:0", **PILE_KW)
+    scenes.build_box_pile(s, nx=nx, ny=ny, nz=nx, seed=seed)
+    return s
+
+
+def generate(n_samples, seed=0, scenes_per_family=200, substeps_per_cloth=8, pile_frames=1, log=print):
+    """Alternates cloths and piles until `n_samples`; each scene contributes a
+    random subset of at most n_samples / (2 scenes_per_family) of its rows, so
+    the samples span many scenes (compliances, sizes, pile heights, times)."""
     rng = np.random.default_rng(seed)
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    per_scene = max(1, n_samples // (2 * scenes_per_family))
     F, T = [], []
-    total = 0
+    got = {"cloth": 0, "pile": 0}
     t0 = time.time()
-    while total < n_samples:
-        n = int(rng.integers(32, 129))
-        comp = float(10.0 ** rng.uniform(-10, -4))
-        s = make_cloth(n, comp)
-        for _ in range(int(rng.integers(0, 40))):
-            s.step()
-        f, t = collect(s, substeps=substeps_per_cloth, iters=50)
+    while got["cloth"] + got["pile"] < n_samples:
+        if got["cloth"] <= got["pile"]:
+            n = int(rng.integers(32, 129))
+            comp = float(10.0 ** rng.uniform(-10, -4))
+            s = make_cloth(n, comp)
+            for _ in range(int(rng.integers(0, 40))):
+                s.step()
+            f, t = collect(s, substeps=substeps_per_cloth, iters=50)
+            kind, what = "cloth", f"cloth {n}x{n} compliance {comp:.2e}"
+        else:
+            k = int(rng.integers(256, 1441))
+            s = make_pile(k, int(rng.integers(1 << 30)))
+            for _ in range(int(rng.integers(30, 300))):
+                s.step()
+            f, t = collect6(s, frames=pile_frames, iters=50)
+            kind, what = "pile", f"pile {s.num_bodies} boxes"
+        if len(t) > per_scene:
+            sel = torch.randperm(len(t), device=t.device, generator=gen)[:per_scene]
+            f, t = f[sel], t[sel]
         F.append(f)
         T.append(t)
-        total += len(t)
-        log(f"  cloth {n}x{n} compliance {comp:.2e}: {len(t)} samples (total {total}, {time.time() - t0:.1f} s)")
+        got[kind] += len(t)
+        log(f"  {what}: {len(t)} samples (cloth {got['cloth']}, pile {got['pile']}, {time.time() - t0:.1f} s)")
     return torch.cat(F)[:n_samples], torch.cat(T)[:n_samples]
 
 
-def train(F, T, epochs=4, batch=8192, lr=2e-3, seed=0, log=print):
+def train(F, T, epochs=40, batch=8192, lr=2e-3, seed=0, log=print):
     torch.manual_seed(seed)
     m = WarmStartMLP(seed=seed)
     n = len(T)
     for ep in range(epochs):
         perm = torch.randperm(n, device=F.device)
-        acc = 0.0
-        steps = 0
+        rate = lr * 0.5 * (1.0 + math.cos(math.pi * ep / epochs))
+        losses = []
         for k in range(0, n, batch):
             sel = perm[k:k + batch]
-            loss = m.train_step(F[sel], T[sel], lr=lr * (0.5 ** ep))
-            if steps % 64 == 0:
-                acc += float(loss.item())
-            steps += 1
-        log(f"  epoch {ep}: mean sampled loss {acc / max(1, (steps + 63) // 64):.5f}")
+            losses.append(m.train_step(F[sel], T[sel], lr=rate))
+        log(f"  epoch {ep}: mean loss {float(torch.stack(losses).mean()):.5f}")
     return m
 
 
-def evaluate(m, n=128, compliance=1e-5, frames=30, samples=8, tol=1e-4, max_iters=100):
+def evaluate_cloth(m, n=128, compliance=1e-5, frames=30, substeps=16, tol=1e-4, max_iters=200):
+    """A hanging n x n cloth after `frames` frames; the next `substeps` substeps
+    one by one (the first has no previous converged multiplier and is left out
+    of the means)."""
     s = make_cloth(n, compliance)
     for _ in range(frames):
         s.step()
-    rows = []
-    for k in range(samples):
-        rows.append(iterations_to_tol(s, m, tol=tol, max_iters=max_iters))
-        s.step()
+    rows = [iterations_to_tol(s, m, tol=tol, max_iters=max_iters, advance=True) for _ in range(substeps)][1:]
     plain = np.array([r["plain"] for r in rows])
     learned = np.array([r["learned_with_fallback"] for r in rows])
-    return {"cloth": f"{n}x{n}", "compliance": compliance, "tol_m": tol, "max_iters": max_iters,
-            "iters_plain": plain.tolist(), "iters_learned": learned.tolist(),
+    pf_plain = np.array([r["to_plain_final"]["plain"] for r in rows])
+    pf_fb = np.array([r["to_plain_final"]["plain"] if r["fallback"] else r["to_plain_final"]["learned"] for r in rows])
+    return {"scene": f"cloth {n}x{n}", "compliance": compliance, "tol_m": tol, "max_iters": max_iters,
+            "substeps": len(rows), "iters_plain": plain.tolist(), "iters_learned": learned.tolist(),
             "fallbacks": int(sum(r["fallback"] for r in rows)),
             "mean_plain": float(plain.mean()), "mean_learned": float(learned.mean()),
-            "ratio": float(plain.mean() / max(learned.mean(), 1e-9))}
+            "ratio": float(plain.mean() / max(learned.mean(), 1e-9)),
+            "iters_to_plain_final": {"plain": float(pf_plain.mean()), "learned_with_fallback": float(pf_fb.mean())},
+            "plain_final_residual_mean": float(np.mean([r["residual_plain"][-1] for r in rows]))}
+
+
+def evaluate_pile(m, frames_before=240, frames=2, tol=1e-4, max_iters=50, seed=0):
+    """The 1440-box pile (12 x 10 x 12, seed 0) after `frames_before` frames; the
+    next `frames` frames substep by substep (the first substep of the run has no
+    previous converged multiplier and is left out of the means)."""
+    s = Solver6DOF(device="cuda:0", **PILE_KW)
+    scenes.build_box_pile(s, seed=seed)
+    for _ in range(frames_before):
+        s.step()
+    kit = SubstepKit6(s)
+    prev = {"classic lambda_prev": (1.0, lambda k: torch.cat([k.prev_floor, k.prev_pair]))}
+    rows = []
+    for f in range(frames):
+        kit.broadphase()
+        for _ in range(s.substeps):
+            rows.append(iterations_to_tol6(kit, m, tol=tol, max_iters=max_iters, variants=prev))
+    rows = rows[1:]
+    pf_plain = np.array([r["to_plain_final"]["plain"] for r in rows])
+    pf_learn = np.array([r["to_plain_final"]["learned"] for r in rows])
+    fb = np.array([r["fallback"] for r in rows])
+    pf_fb = np.where(fb, pf_plain, pf_learn)
+    pf_prev = np.array([r["classic lambda_prev"]["to_plain_final"] for r in rows])
+    res2 = {"plain": float(np.mean([r["residual_plain"][1] for r in rows])),
+            "learned": float(np.mean([r["residual_learned"][1] for r in rows])),
+            "classic lambda_prev": float(np.mean([r["classic lambda_prev"]["second"] for r in rows]))}
+    return {"scene": f"box pile {s.num_bodies} after {frames_before} frames", "substeps": len(rows),
+            "tol_m": tol, "max_iters": max_iters,
+            "iters_to_tol": {"plain": float(np.mean([r["plain"] for r in rows])),
+                             "learned_with_fallback": float(np.mean([r["learned_with_fallback"] for r in rows]))},
+            "plain_final_residual_mean": float(np.mean([r["residual_plain"][-1] for r in rows])),
+            "iters_to_plain_final": {"plain": float(pf_plain.mean()), "learned": float(pf_learn.mean()),
+                                     "learned_with_fallback": float(pf_fb.mean()),
+                                     "classic lambda_prev": float(pf_prev.mean())},
+            "fallbacks": int(fb.sum()), "mean_residual_after_2_iters": res2,
+            "ratio_with_fallback": float(pf_plain.mean() / max(pf_fb.mean(), 1e-9))}
+
+
+def _event_ms(fn, reps=20):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fn()
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def time_warm_start(m):
+    """Device time of the warm start's extra work per substep (features +
+    inference + warm apply) against one plain Jacobi iteration (solve + apply),
+    on the 1440-box pile after 240 frames and on the 128 x 128 cloth; each is
+    repeated from the same state."""
+    from .learned import SubstepKit
+    out = {}
+    s = Solver6DOF(device="cuda:0", **PILE_KW)
+    scenes.build_box_pile(s)
+    for _ in range(240):
+        s.step()
+    kit = SubstepKit6(s)
+    kit.broadphase()
+    kit.begin()
+    snap = kit.snapshot()
+    rows = int((kit.weff > 0).sum().item())
+
+    def warm6():
+        kit.restore(snap)
+        N6 = kit.L
+        from . import _native as N
+        N.check(N6.xpbd6_features(kit.st, kit.par, N.ptr(kit.prev_floor), N.ptr(kit.prev_pair), N.ptr(kit.feats),
+                                  N.ptr(kit.weff), kit.stream()))
+        kit.warm(m)
+
+    def iter6():
+        kit.restore(snap)
+        kit.iterate()
+    out["pile"] = {"rows": rows, "warm_start_ms": round(_event_ms(warm6), 4),
+                   "iteration_ms": round(_event_ms(iter6), 4)}
+    c = make_cloth(128, 1e-5)
+    for _ in range(30):
+        c.step()
+    ck = SubstepKit(c)
+    snap3 = c.state_dict()
+    ck.integrate()
+
+    def warm3():
+        ck.features()
+        ck.warm(m)
+
+    def iter3():
+        ck.iterate(first=False)
+    rows3 = int(c.tensors["n_rows"].item())
+    out["cloth"] = {"rows": rows3, "warm_start_ms": round(_event_ms(warm3), 4),
+                    "iteration_ms": round(_event_ms(iter3), 4)}
+    c.load_state_dict(snap3)
+    return out
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--samples", type=int, default=10_000_000)
-    ap.add_argument("--epochs", type=int, default=4)
-    ap.add_argument("--out", default=None)
-    ap.add_argument("--eval", default=None, help="evaluate a saved model instead of training")
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--out", default=None, help="save the trained weights (float32 .npy)")
+    ap.add_argument("--eval", default=None, help="evaluate saved weights instead of training")
     ap.add_argument("--seed", type=int, default=0)
     a = ap.parse_args()
+    report = {}
     if a.eval:
         m = WarmStartMLP()
-        m.load_state_dict(torch.load(a.eval))
+        m.load_weights(a.eval)
     else:
         t0 = time.time()
         F, T = generate(a.samples, seed=a.seed)
-        print(f"generated {len(T)} samples in {time.time() - t0:.1f} s")
+        report["samples"] = len(T)
+        report["generate_s"] = round(time.time() - t0, 1)
         t0 = time.time()
         m = train(F, T, epochs=a.epochs, seed=a.seed)
-        print(f"trained in {time.time() - t0:.1f} s")
+        torch.cuda.synchronize()
+        report["train_s"] = round(time.time() - t0, 1)
+        report["epochs"] = a.epochs
         if a.out:
-            torch.save(m.state_dict(), a.out)
-    print(json.dumps(evaluate(m)))
+            m.save_weights(a.out)
+    report["cloth"] = evaluate_cloth(m)
+    report["cloth_c1e-4"] = evaluate_cloth(m, compliance=1e-4)
+    report["pile"] = evaluate_pile(m)
+    report["timing"] = time_warm_start(m)
+    print(json.dumps(report))
 
 
 if __name__ == "__main__":
