@@ -306,6 +306,12 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
         torch.cuda.synchronize(device)
     frame_ms = [a.elapsed_time(c) for a, _, c in ev]
     kern_ms = [b.elapsed_time(c) for _, b, c in ev]
+    # rows of the last timed frame (before anything else advances the pile)
+    n = s.num_bodies
+    n_dyn = int((s.tensors["x"][:, 3] > 0).sum().item())
+    npairs = min(s.n_pairs, s.cap)
+    hdr = s.tensors["m_hdr"][:npairs].cpu().numpy()
+    points = int(hdr[:, 0].sum())
     # graph replay of the whole frame (broad phase + substeps), back to back
     g0 = torch.cuda.Event(enable_timing=True)
     g1 = torch.cuda.Event(enable_timing=True)
@@ -315,11 +321,6 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
     torch.cuda.synchronize(device)
     graph_ms = g0.elapsed_time(g1) / args.steps
     status = s.status()
-    n = s.num_bodies
-    n_dyn = int((s.tensors["x"][:, 3] > 0).sum().item())
-    npairs = min(s.n_pairs, s.cap)
-    hdr = s.tensors["m_hdr"][:npairs].cpu().numpy()
-    points = int(hdr[:, 0].sum())
     rows = 8 * n_dyn + points + s.num_joints
     proj_per_frame = rows * s.substeps * s.iterations
     S, I = s.substeps, s.iterations
@@ -359,9 +360,9 @@ def time_e2e(args, workload, device):
             host[k].copy_(T[k], non_blocking=True)
         stream.synchronize()
 
-    for _ in range(max(3, args.warmup)):
+    for _ in range(max(3, args.warmup)):  # the same frames as the device-timed leg
         frame()
-    steps = max(1, args.steps // 2)
+    steps = args.steps
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)

@@ -13,7 +13,7 @@ lambda0, instead of from lambda = 0.
 The plain solve stays the fallback: in ``WarmStartRunner`` every substep runs the
 first iteration both ways and keeps the plain one whenever its residual is not
 worse than the learned one's.  The residual (``Solver.residual``) -- hard rows
-max(0, -C), compliant rows |C + alpha~ lambda| -- is the judge of both.
+max(0, -C), compliant rows |C + alpha~ lambda| -- decides between them.
 """
 
 from __future__ import annotations
