@@ -173,6 +173,35 @@ def test_sphere_contacts_2048_bit_exact(golden):
     assert np.all(r["type"][k:] == 3)
 
 
+@pytest.mark.parametrize("dims", [(16, 8, 16), (20, 12, 20)], ids=["fused_2048", "multi_kernel_4800"])
+def test_sphere_contacts_match_oracle_both_paths(dims):
+    """Contact rows for a jittered, overlapping pile with random velocities (so
+    the velocity margin matters), against the oracle's restatement of
+    solver.py:275-342: up to 4096 collidable spheres the single-CTA fused
+    builder runs, above it the multi-kernel one; both bit for bit."""
+    nx, ny, nz = dims
+    kw = dict(dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi")
+    s = Solver(device="cuda:0", **kw)
+    o = O.OracleSolver(device="cpu", **kw)
+    for t in (s, o):
+        scenes.build_sphere_pile(t, nx=nx, ny=ny, nz=nz, pitch=0.098, seed=3)
+    s._flush()
+    o._flush()
+    v = np.random.default_rng(1).normal(size=(s.num_bodies, 3)).astype(np.float32)
+    s.tensors["v"][:, :3] = torch.from_numpy(v).cuda()
+    o.v[:] = v
+    s._build_contacts(N.stream_of(s.device))
+    o._rebuild_contacts()
+    r = s.rows()
+    k = s._n_static
+    want = [row for row in o._rows if row.type == 3]
+    assert len(want) > 4 * s.num_bodies
+    np.testing.assert_array_equal(r["a"][k:], np.array([row.body_a for row in want]))
+    np.testing.assert_array_equal(r["b"][k:], np.array([row.body_b for row in want]))
+    np.testing.assert_array_equal(r["rest"][k:], np.array([row.rest for row in want], np.float32))
+    np.testing.assert_array_equal(r["mu"][k:], np.array([row.mu for row in want], np.float32))
+
+
 def test_nan_positions_are_reset_and_flagged():
     s = Solver(device="cuda:0", dt=1 / 60, substeps=4, iterations=1, solve_mode="jacobi")
     scenes.build_sphere_pile(s, nx=2, ny=2, nz=2, pitch=0.12, y0=0.3)

@@ -231,6 +231,263 @@ __global__ void kc_write(ContactArgs a, ContactScratch s) {
   }
 }
 
+// ---- fused cluster builder -------------------------------------------------------
+// For up to kFusedMaxCollide collidable spheres the whole build is one launch of
+// one thread-block cluster (up to 16 CTAs of 1024 threads):
+//  * every CTA redundantly loads the sanitized positions, reduces max |v| and the
+//    cell bounds, and sorts the cell keys in its own shared memory (stable radix
+//    sort), so no communication is needed up to this point; only rank 0 writes
+//    the reset positions back and raises the status bit;
+//  * the 14 m (offset, sphere) slots, in emission order, are split into one
+//    contiguous range per CTA and one sub-range per thread; each thread counts
+//    its slots (a one-bit-per-slot mask remembers the non-empty ones), a block
+//    scan gives the thread offsets, and each CTA's base is the sum of the
+//    totals of the CTAs before it, read through distributed shared memory after
+//    one cluster barrier;
+//  * each thread then re-walks its slots and writes their rows.
+// The rows are identical to the multi-kernel path's.
+constexpr int kFusedMaxCollide = 4096;
+
+struct FusedView {
+  uint64_t* skey;  // sorted cid
+  uint32_t* sval;  // sorted local index
+  float4* pos;     // per collidable: sanitized position, radius
+};
+
+static inline size_t fused_smem_bytes(int m) {
+  return (size_t)m * (2 * sizeof(uint64_t) + 2 * sizeof(uint32_t) + sizeof(float4)) +
+         sizeof(unsigned) * (size_t)((14 * m + 31) / 32);
+}
+
+XD int lower_bound_smem(const uint64_t* s, int m, uint64_t t) {
+  int lo = 0, hi = m;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (s[mid] < t) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// visit_slot with the sorted keys and positions read from shared memory.
+template <class Emit>
+XD int visit_slot_fused(const ContactArgs& a, const FusedView& f, int o, int k, int64_t cid_k, float margin_f,
+                        int64_t S, Emit emit) {
+  int64_t delta = ((int64_t)kFwd[o][0] * S + kFwd[o][1]) * S + kFwd[o][2];
+  int64_t target = cid_k + delta;
+  if (target < 0) return 0;
+  int q = lower_bound_smem(f.skey, a.m, (uint64_t)target);
+  int cnt = 0;
+  const int ga = a.coll[k];
+  const float4 pa = f.pos[k];
+  for (; q < a.m && f.skey[q] == (uint64_t)target; ++q) {
+    int partner = (int)f.sval[q];
+    if (o == 0 && !(partner > k)) continue;
+    const float4 pb = f.pos[partner];
+    float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
+    float d2 = dx * dx + dy * dy + dz * dz;
+    float rs = pa.w + pb.w + margin_f;
+    if (!(d2 <= rs * rs)) continue;
+    int gb = a.coll[partner];
+    if (a.n_existing) {
+      int64_t key = ga < gb ? (int64_t)ga * a.n + gb : (int64_t)gb * a.n + ga;
+      if (has_key(a.existing, a.n_existing, key)) continue;
+    }
+    emit(cnt, ga, gb);
+    ++cnt;
+  }
+  return cnt;
+}
+
+XD unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+XD unsigned cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+XD void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// Loads an int from the shared memory of CTA `rank` of this cluster.
+XD int ld_cluster_int(const int* local, unsigned rank) {
+  unsigned addr = (unsigned)__cvta_generic_to_shared(local), remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(addr), "r"(rank));
+  int v;
+  asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(remote) : "memory");
+  return v;
+}
+
+__global__ void __launch_bounds__(1024) kc_fused(ContactArgs a) {
+  extern __shared__ __align__(16) unsigned char fused_dyn[];
+  __shared__ BlockSortSmem sort_sm;
+  __shared__ int s_min[3], s_max[3], s_vmax_bits;
+  __shared__ int s_warp[32];
+  __shared__ int s_cta_total;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned rank = cluster_rank(), csize = cluster_size();
+  const int m = a.m;
+  FusedView f;
+  f.skey = reinterpret_cast<uint64_t*>(fused_dyn);
+  uint64_t* skey2 = f.skey + m;
+  f.pos = reinterpret_cast<float4*>(skey2 + m);
+  f.sval = reinterpret_cast<uint32_t*>(f.pos + m);
+  uint32_t* sval2 = f.sval + m;
+  unsigned* nonempty = sval2 + m;
+  if (tid < 3) {
+    s_min[tid] = 0x7fffffff;
+    s_max[tid] = (int)0x80000000;
+  }
+  if (tid == 0) s_vmax_bits = 0;
+  __syncthreads();
+  // 1. solver.py:469-483 sanitize, and the max |v| of solver.py:309 over the
+  // sanitized velocities.  Every CTA works on the sanitized values without
+  // writing them; rank 0 writes them back once no CTA reads x or v any more
+  // (after the first cluster barrier below).
+  float vm = 0.0f;
+  for (int i = tid; i < a.n; i += 1024) {
+    float4 vi = a.v[i];
+    if (!finite3(a.x[i])) vi = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    vm = fmaxf(vm, fmaxf(fabsf(vi.x), fmaxf(fabsf(vi.y), fabsf(vi.z))));
+  }
+  for (int o = 16; o; o >>= 1) vm = fmaxf(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+  if (lane == 0) atomicMax(&s_vmax_bits, __float_as_int(vm));
+  __syncthreads();
+  if (m < 2) {  // uniform across the cluster: every CTA returns here
+    if (rank == 0) {
+      for (int i = tid; i < a.n; i += 1024) {
+        float4 xi = a.x[i];
+        if (!finite3(xi)) {
+          float4 x0 = a.x_init[i];
+          a.x[i] = make_float4(x0.x, x0.y, x0.z, xi.w);
+          a.v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          raise_status(a.status, XPBD_ERR_NAN);
+        }
+      }
+      if (tid == 0) *a.n_rows = a.n_static;
+    }
+    return;
+  }
+  ContactRed red;
+  red.vmax_bits = s_vmax_bits;
+  float cell, marg;
+  margin_cell(a, &red, &cell, &marg);
+  // 2. cell bounds over the sanitized positions
+  int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (int k = tid; k < m; k += 1024) {
+    const int g = a.coll[k];
+    float4 p = a.x[g];
+    if (!finite3(p)) p = a.x_init[g];
+    f.pos[k] = make_float4(p.x, p.y, p.z, a.radius[g]);
+    int c[3] = {(int)floorf(p.x / cell), (int)floorf(p.y / cell), (int)floorf(p.z / cell)};
+    for (int d = 0; d < 3; ++d) {
+      lmin[d] = min(lmin[d], c[d]);
+      lmax[d] = max(lmax[d], c[d]);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o; o >>= 1) {
+      lmin[d] = min(lmin[d], __shfl_xor_sync(0xffffffffu, lmin[d], o));
+      lmax[d] = max(lmax[d], __shfl_xor_sync(0xffffffffu, lmax[d], o));
+    }
+    if (lane == 0) {
+      atomicMin(&s_min[d], lmin[d]);
+      atomicMax(&s_max[d], lmax[d]);
+    }
+  }
+  for (int i = tid; i < (14 * m + 31) / 32; i += 1024) nonempty[i] = 0u;
+  __syncthreads();
+  for (int d = 0; d < 3; ++d) {
+    red.cmin[d] = s_min[d];
+    red.cmax[d] = s_max[d];
+  }
+  const int64_t S = grid_S(&red);
+  auto cid_of = [&](int k) {
+    float4 p = f.pos[k];
+    int64_t cx = (int64_t)(int)floorf(p.x / cell) - red.cmin[0], cy = (int64_t)(int)floorf(p.y / cell) - red.cmin[1],
+            cz = (int64_t)(int)floorf(p.z / cell) - red.cmin[2];
+    return (cx * S + cy) * S + cz;
+  };
+  // 3. keys, 4. stable sort (ties keep ascending index)
+  for (int k = tid; k < m; k += 1024) {
+    f.skey[k] = (uint64_t)cid_of(k);
+    f.sval[k] = (uint32_t)k;
+  }
+  __syncthreads();
+  block_sort_pairs_u64(sort_sm, f.skey, f.sval, skey2, sval2, m, 63);
+  // 5. count this thread's slots (slot t = o m + k) within this CTA's range
+  const int slots = 14 * m;
+  const int per_cta = (slots + (int)csize - 1) / (int)csize;
+  const int c0 = min((int)rank * per_cta, slots), c1 = min(c0 + per_cta, slots);
+  const int per = (c1 - c0 + 1023) / 1024;
+  const int t0 = min(c0 + tid * per, c1), t1 = min(t0 + per, c1);
+  int mine = 0;
+  for (int t = t0; t < t1; ++t) {
+    const int o = t / m, k = t - o * m;
+    int c = visit_slot_fused(a, f, o, k, cid_of(k), marg, S, [](int, int, int) {});
+    if (c) atomicOr(&nonempty[t >> 5], 1u << (t & 31));
+    mine += c;
+  }
+  int inc = mine;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    int w = s_warp[lane];
+    int wi = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    s_warp[lane] = wi - w;
+    if (lane == 31) s_cta_total = wi;
+  }
+  cluster_sync_all();  // every CTA's total is visible, and no CTA reads x or v any more
+  if (rank == 0) {
+    for (int i = tid; i < a.n; i += 1024) {
+      float4 xi = a.x[i];
+      if (!finite3(xi)) {
+        float4 x0 = a.x_init[i];
+        a.x[i] = make_float4(x0.x, x0.y, x0.z, xi.w);
+        a.v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        raise_status(a.status, XPBD_ERR_NAN);
+      }
+    }
+  }
+  int cta_base = 0, total = 0;
+  for (unsigned q = 0; q < csize; ++q) {
+    int tq = ld_cluster_int(&s_cta_total, q);
+    if (q < rank) cta_base += tq;
+    total += tq;
+  }
+  cluster_sync_all();  // no CTA leaves while another may still read its total
+  int base = cta_base + s_warp[warp] + inc - mine;
+  if (rank == 0 && tid == 0) {
+    *a.n_rows = a.n_static + min(total, a.cap_contacts);
+    if (total > a.cap_contacts) raise_status(a.status, XPBD_ERR_OVERFLOW);
+  }
+  // 6. write the rows of this thread's slots at their offsets
+  for (int t = t0; t < t1; ++t) {
+    if (!(nonempty[t >> 5] & (1u << (t & 31)))) continue;
+    const int o = t / m, k = t - o * m;
+    const int b0 = base;
+    base += visit_slot_fused(a, f, o, k, cid_of(k), marg, S, [&](int r, int ga, int gb) {
+      int slot = b0 + r;
+      if (slot >= a.cap_contacts) return;
+      int row = a.n_static + slot;
+      a.ri[row] = make_int4(XPBD_CONTACT, ga, gb, 1);
+      a.rf[row] = make_float4(a.radius[ga] + a.radius[gb], 0.0f, sqrtf(a.friction[ga] * a.friction[gb]), 0.0f);
+      a.ra[row] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    });
+  }
+}
+
 __global__ void kc_no_contacts(ContactArgs a) {
   if (gtid() == 0) *a.n_rows = a.n_static;
 }
@@ -238,6 +495,43 @@ __global__ void kc_no_contacts(ContactArgs a) {
 }  // namespace xpbd
 
 using namespace xpbd;
+
+// Cluster size of the fused builder on the current device (largest of 16, 8,
+// 4, 2, 1 CTAs with the maximum shared memory that the device can co-schedule;
+// 0 = the fused builder cannot run), chosen once per device.
+static int fused_cluster_size(int* out) {
+  static int chosen[64];
+  static bool done[64] = {false};
+  int dev = 0;
+  XPBD_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return XPBD_ERR_BAD_ARG;
+  if (!done[dev]) {
+    const size_t smem = fused_smem_bytes(kFusedMaxCollide);
+    XPBD_CUDA(cudaFuncSetAttribute(kc_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    XPBD_CUDA(cudaFuncSetAttribute(kc_fused, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    int pick = 0;
+    for (int c = 16; c >= 1 && !pick; c /= 2) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(c);
+      cfg.blockDim = dim3(1024);
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = c;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, kc_fused, &cfg) == cudaSuccess && n > 0) pick = c;
+      cudaGetLastError();
+    }
+    chosen[dev] = pick;
+    done[dev] = true;
+  }
+  *out = chosen[dev];
+  return XPBD_OK;
+}
 
 struct xpbd3_contacts {
   int n = 0, m = 0;
@@ -320,6 +614,27 @@ extern "C" int xpbd3_contacts_build(xpbd3_contacts* c, const xpbd3_state* st, co
   a.cap_contacts = st->row_capacity - st->n_rows_static;
   a.status = status_dev;
   if (a.n == 0) return XPBD_OK;
+  if (a.m <= kFusedMaxCollide) {
+    int csize = 0;
+    int rc = fused_cluster_size(&csize);
+    if (rc) return rc;
+    if (csize > 0) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(csize);
+      cfg.blockDim = dim3(1024);
+      cfg.dynamicSmemBytes = fused_smem_bytes(a.m);
+      cfg.stream = s;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = csize;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      XPBD_CUDA(cudaLaunchKernelEx(&cfg, kc_fused, a));
+      return XPBD_OK;
+    }
+  }
   kc_init<<<1, 32, 0, s>>>(c->s.red);
   kc_sanitize<<<stream_blocks(a.n, 256), 256, 0, s>>>(a, c->s.red);
   if (a.m < 2) {

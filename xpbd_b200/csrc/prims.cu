@@ -14,90 +14,8 @@ constexpr unsigned kFull = 0xffffffffu;
 
 __global__ void __launch_bounds__(1024) k_radix_sort_block(uint64_t* k0, uint32_t* v0, uint64_t* k1,
                                                            uint32_t* v1, int n, int max_bits) {
-  __shared__ unsigned hist[256];
-  __shared__ unsigned base[256];
-  __shared__ unsigned wcnt[32][257];
-  __shared__ unsigned long long smax;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) smax = 0ull;
-  __syncthreads();
-  unsigned long long mk = 0ull;
-  for (int i = tid; i < n; i += 1024) mk = max(mk, (unsigned long long)k0[i]);
-  for (int o = 16; o; o >>= 1) mk = max(mk, __shfl_xor_sync(kFull, mk, o));
-  if (lane == 0) atomicMax(&smax, mk);
-  __syncthreads();
-  int bits = smax ? 64 - __clzll((long long)smax) : 0;
-  if (bits > max_bits) bits = max_bits;
-  const int passes = (bits + 7) / 8;
-  uint64_t *ks = k0, *kd = k1;
-  uint32_t *vs = v0, *vd = v1;
-  for (int p = 0; p < passes; ++p) {
-    const int shift = 8 * p;
-    if (tid < 256) hist[tid] = 0;
-    __syncthreads();
-    for (int i = tid; i < n; i += 1024) atomicAdd(&hist[(unsigned)((ks[i] >> shift) & 255ull)], 1u);
-    __syncthreads();
-    if (tid < 32) {
-      unsigned s[8], tot = 0;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        s[q] = hist[lane * 8 + q];
-        tot += s[q];
-      }
-      unsigned inc = tot;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        unsigned y = __shfl_up_sync(kFull, inc, o);
-        if (lane >= o) inc += y;
-      }
-      unsigned run = inc - tot;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        base[lane * 8 + q] = run;
-        run += s[q];
-      }
-    }
-    __syncthreads();
-    for (int start = 0; start < n; start += 1024) {
-      const int i = start + tid;
-      const bool valid = i < n;
-      const uint64_t key = valid ? ks[i] : 0ull;
-      const uint32_t val = valid ? vs[i] : 0u;
-      const unsigned d = valid ? (unsigned)((key >> shift) & 255ull) : 256u;
-      for (int q = tid; q < 32 * 257; q += 1024) (&wcnt[0][0])[q] = 0u;
-      __syncthreads();
-      const unsigned peers = __match_any_sync(kFull, d);
-      const unsigned rank = __popc(peers & ((1u << lane) - 1u));
-      if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
-      __syncthreads();
-      if (tid < 256) {
-        unsigned run = 0;
-        for (int w = 0; w < 32; ++w) {
-          unsigned c = wcnt[w][tid];
-          wcnt[w][tid] = run;
-          run += c;
-        }
-        hist[tid] = run;
-      }
-      __syncthreads();
-      if (valid) {
-        unsigned pos = base[d] + wcnt[warp][d] + rank;
-        kd[pos] = key;
-        vd[pos] = val;
-      }
-      __syncthreads();
-      if (tid < 256) base[tid] += hist[tid];
-      __syncthreads();
-    }
-    uint64_t* tk = ks; ks = kd; kd = tk;
-    uint32_t* tv = vs; vs = vd; vd = tv;
-  }
-  if (passes & 1) {
-    for (int i = tid; i < n; i += 1024) {
-      k0[i] = ks[i];
-      v0[i] = vs[i];
-    }
-  }
+  __shared__ BlockSortSmem S;
+  block_sort_pairs_u64(S, k0, v0, k1, v1, n, max_bits);
 }
 
 size_t sort_scratch_bytes(int n) { return (size_t)(n > 0 ? n : 1) * (sizeof(uint64_t) + sizeof(uint32_t)) + 16; }
