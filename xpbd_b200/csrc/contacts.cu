@@ -298,29 +298,6 @@ XD int visit_slot_fused(const ContactArgs& a, const FusedView& f, int o, int k, 
   return cnt;
 }
 
-XD unsigned cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-XD unsigned cluster_size() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-  return r;
-}
-XD void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
-  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
-}
-// Loads an int from the shared memory of CTA `rank` of this cluster.
-XD int ld_cluster_int(const int* local, unsigned rank) {
-  unsigned addr = (unsigned)__cvta_generic_to_shared(local), remote;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(addr), "r"(rank));
-  int v;
-  asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(remote) : "memory");
-  return v;
-}
-
 __global__ void __launch_bounds__(1024) kc_fused(ContactArgs a) {
   extern __shared__ __align__(16) unsigned char fused_dyn[];
   __shared__ BlockSortSmem sort_sm;

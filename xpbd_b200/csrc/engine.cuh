@@ -110,4 +110,55 @@ XD void grid_sync(const GridBarrier& b) {
 XD int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 XD int gstride() { return gridDim.x * blockDim.x; }
 
+// thread-block cluster helpers (one-cluster launches)
+XD unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+XD unsigned cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+XD void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// Loads an int from the shared memory of CTA `rank` of this cluster.
+XD int ld_cluster_int(const int* local, unsigned rank) {
+  unsigned addr = (unsigned)__cvta_generic_to_shared(local), remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(addr), "r"(rank));
+  int v;
+  asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(remote) : "memory");
+  return v;
+}
+// Block-wide exclusive scan of one int per thread (blockDim.x <= 1024, a
+// multiple of 32); `sh` is 33 ints of shared memory.  Returns the thread's
+// exclusive prefix and writes the block total to *total on every thread.
+XD int block_exclusive_scan(int v, int* sh, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  __syncthreads();  // sh may still be read by a previous call
+  if (lane == 31) sh[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < nw ? sh[lane] : 0;
+    int wi = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    sh[lane] = wi - w;
+    if (lane == 31) sh[32] = wi;
+  }
+  __syncthreads();
+  *total = sh[32];
+  return sh[warp] + inc - v;
+}
+
 }  // namespace xpbd

@@ -1313,6 +1313,329 @@ __global__ void k6_pairs_write(Dev6 s, BP6 b, int* status) {
 }
 
 // =================================================================================
+// Fused LBVH broad phase for one scene of up to kFusedMaxBoxes bodies: one launch
+// of one thread-block cluster (up to 16 CTAs of 1024 threads).  Every CTA builds
+// the whole tree in its own shared memory -- body AABBs, Morton keys, stable
+// radix sort, Karras build, bottom-up refit -- so no communication is needed up
+// to here; the queries are split: each CTA takes a contiguous range of bodies,
+// each thread a sub-range, counts its pairs, and the offsets come from a block
+// scan plus the totals of the CTAs before it (distributed shared memory, after
+// one cluster barrier).  The pair list equals the multi-kernel path's (the pair
+// set depends only on the inclusive box tests, each body's pairs are sorted by
+// j, bodies are in ascending order).
+// =================================================================================
+constexpr int kFusedMaxBoxes = 2048;
+constexpr int kFrontierRounds = 3;  // 2^3 = 8 lanes per query
+
+// Shared memory: lo, hi (2 x 16 n), region A (32 n: sort keys + ping-pong
+// during the sort and build, internal-node bounds afterwards), child (8 n),
+// parent (8 n), flags (4 n), vals (4 n).
+constexpr int kStagePairs = 32;  // per-group staging of one body's pairs for the sort
+static inline size_t bp_fused_smem(int n) {
+  return (size_t)n * (32 + 32 + 4 + 8 + 8 + 4) + sizeof(int) * (size_t)(1024 / 8) * kStagePairs;
+}
+// bodies per 8-lane group: ceil(ceil(n / cluster) / 128) <= 16 for n <= 2048
+constexpr int kMaxGroupBodies = 16;
+
+// shared-memory float4 access that the compiler may not cache (refit hand-off)
+XD float4 ld_vol4(const float4* p) {
+  const volatile float* q = reinterpret_cast<const volatile float*>(p);
+  return make_float4(q[0], q[1], q[2], q[3]);
+}
+XD void st_vol4(float4* p, float4 v) {
+  volatile float* q = reinterpret_cast<volatile float*>(p);
+  q[0] = v.x;
+  q[1] = v.y;
+  q[2] = v.z;
+  q[3] = v.w;
+}
+
+__global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts, int* status) {
+  extern __shared__ __align__(16) unsigned char bp_dyn[];
+  __shared__ BlockSortSmem sort_sm;
+  __shared__ int s_bounds[6];
+  __shared__ int s_scan[33];
+  const int n = s.n, tid = threadIdx.x, T = blockDim.x;
+  const unsigned rank = cluster_rank(), csize = cluster_size();
+  float4* LO = reinterpret_cast<float4*>(bp_dyn);
+  float4* HI = LO + n;
+  unsigned char* regionA = reinterpret_cast<unsigned char*>(HI + n);
+  uint64_t* keys = reinterpret_cast<uint64_t*>(regionA);
+  uint64_t* keys2 = keys + n;
+  uint32_t* vals2 = reinterpret_cast<uint32_t*>(keys2 + n);
+  float4* INLO = reinterpret_cast<float4*>(regionA);  // after the build
+  float4* INHI = INLO + n;
+  int2* child = reinterpret_cast<int2*>(regionA + 32 * (size_t)n);  // 8-byte aligned for any n
+  int* parent = reinterpret_cast<int*>(child + n);
+  int* flags = parent + 2 * n;
+  uint32_t* vals = reinterpret_cast<uint32_t*>(flags + n);
+  int* stage_all = reinterpret_cast<int*>(vals + n);  // [1024 / 8][kStagePairs]
+  if (tid < 3) {
+    s_bounds[tid] = 0x7fffffff;
+    s_bounds[3 + tid] = (int)0x80000000;
+  }
+  __syncthreads();
+  // 1. kernels_bvh.py:22-48 body AABBs + bounds of their centres
+  int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (int i = tid; i < n; i += T) {
+    body_aabb(s, i, p.margin, p.dt, LO, HI);
+    // the unused w lanes carry what the pair filter needs: inverse mass, group
+    LO[i].w = s.x[i].w;
+    HI[i].w = __int_as_float(s.group[i]);
+    float4 l = LO[i], h = HI[i];
+    float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+    for (int d = 0; d < 3; ++d) {
+      lmin[d] = min(lmin[d], ord_f(c[d]));
+      lmax[d] = max(lmax[d], ord_f(c[d]));
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o; o >>= 1) {
+      lmin[d] = min(lmin[d], __shfl_xor_sync(0xffffffffu, lmin[d], o));
+      lmax[d] = max(lmax[d], __shfl_xor_sync(0xffffffffu, lmax[d], o));
+    }
+    if ((tid & 31) == 0) {
+      atomicMin(&s_bounds[d], lmin[d]);
+      atomicMax(&s_bounds[3 + d], lmax[d]);
+    }
+  }
+  __syncthreads();
+  // 2. Morton keys (the definition of k6_morton)
+  {
+    float cmin[3], inv[3];
+    for (int d = 0; d < 3; ++d) {
+      cmin[d] = unord_f(s_bounds[d]);
+      float ext = unord_f(s_bounds[3 + d]) - cmin[d];
+      inv[d] = ext > 0.0f ? 1.0f / ext : 0.0f;
+    }
+    for (int i = tid; i < n; i += T) {
+      float4 l = LO[i], h = HI[i];
+      float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+      uint32_t k = 0;
+      for (int d = 0; d < 3; ++d) k |= expand10(quant10((c[d] - cmin[d]) * inv[d])) << (2 - d);
+      keys[i] = (uint64_t)k;
+      vals[i] = (uint32_t)i;
+    }
+  }
+  __syncthreads();
+  // 3. stable sort
+  block_sort_pairs_u64(sort_sm, keys, vals, keys2, vals2, n, 30);
+  // 4. Karras build (as k6_build)
+  for (int i = tid; i < n - 1; i += T) {
+    int d = (lbvh_delta(keys, n, i, i + 1) - lbvh_delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = lbvh_delta(keys, n, i, i - d);
+    int lmx = 2;
+    while (lbvh_delta(keys, n, i, i + lmx * d) > dmin) lmx *= 2;
+    int l = 0;
+    for (int t = lmx / 2; t >= 1; t /= 2)
+      if (lbvh_delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = lbvh_delta(keys, n, i, j);
+    int sp = 0;
+    for (int div = 2;; div *= 2) {
+      int t = (l + div - 1) / div;
+      if (lbvh_delta(keys, n, i, i + (sp + t) * d) > dnode) sp += t;
+      if (t <= 1) break;
+    }
+    int gamma = i + sp * d + min(d, 0);
+    int left = (min(i, j) == gamma) ? (n - 1 + gamma) : gamma;
+    int right = (max(i, j) == gamma + 1) ? (n - 1 + gamma + 1) : gamma + 1;
+    child[i] = make_int2(left, right);
+    parent[left] = i;
+    parent[right] = i;
+    flags[i] = 0;
+  }
+  if (tid == 0) parent[0] = -1;
+  __syncthreads();  // the keys are dead: region A now holds the internal bounds
+  // 5. bottom-up refit: the second child to arrive at a node writes its union
+  auto node_lo = [&](int x) -> float4 {
+    return x >= n - 1 ? LO[vals[x - (n - 1)]] : ld_vol4(INLO + x);
+  };
+  auto node_hi = [&](int x) -> float4 {
+    return x >= n - 1 ? HI[vals[x - (n - 1)]] : ld_vol4(INHI + x);
+  };
+  for (int k = tid; k < n; k += T) {
+    int cur = parent[n - 1 + k];
+    for (int depth = 0; cur >= 0; ++depth) {
+      if (depth >= kMaxDepth || cur >= n - 1) {
+        raise_status(status, XPBD_ERR_BAD_INDEX);
+        break;
+      }
+      __threadfence_block();
+      if (atomicAdd(&flags[cur], 1) == 0) break;
+      __threadfence_block();
+      int2 c = child[cur];
+      float4 l0 = node_lo(c.x), l1 = node_lo(c.y), h0 = node_hi(c.x), h1 = node_hi(c.y);
+      st_vol4(INLO + cur, make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f));
+      st_vol4(INHI + cur, make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f));
+      cur = parent[cur];
+    }
+  }
+  __syncthreads();
+  // 6. queries (kernels_bvh.py:52-85): eight lanes per body, each walking one
+  // of the (up to eight) subtrees three levels below the root.  A node's
+  // bounds contain its leaves', so the pairs found are exactly those of a walk
+  // from the root.
+  // keep_pair (kernels_bvh.py:74-83) from the w lanes of the AABBs (one scene)
+  auto keep = [&](int i, int j) {
+    if (!(j > i)) return false;
+    if (LO[i].w == 0.0f && LO[j].w == 0.0f) return false;
+    int gi = __float_as_int(HI[i].w);
+    return !(gi == __float_as_int(HI[j].w) && gi > 0);
+  };
+  // after the refit's barrier the bounds are final: plain vector loads
+  auto qlo_of = [&](int x) -> float4 { return x >= n - 1 ? LO[vals[x - (n - 1)]] : INLO[x]; };
+  auto qhi_of = [&](int x) -> float4 { return x >= n - 1 ? HI[vals[x - (n - 1)]] : INHI[x]; };
+  // walk of the subtree under `start`
+  auto query_from = [&](int i, int start, auto emit) {
+    if (start < 0 || start >= 2 * n - 1) return;
+    const float4 qlo = LO[i], qhi = HI[i];
+    if (!overlaps(qlo, qhi, qlo_of(start), qhi_of(start))) return;
+    if (start >= n - 1) {
+      int j = (int)vals[start - (n - 1)];
+      if (keep(i, j)) emit(j);
+      return;
+    }
+    int stack[kStack];
+    int sp = 0, node = start;
+    for (int visits = 0;; ++visits) {
+      if (visits >= n) {
+        raise_status(status, XPBD_ERR_BAD_INDEX);
+        return;
+      }
+      int2 c = child[node];
+      int ch[2] = {c.x, c.y};
+      for (int e = 0; e < 2; ++e) {
+        int x = ch[e];
+        if (x < 0 || x >= 2 * n - 1) {
+          raise_status(status, XPBD_ERR_BAD_INDEX);
+          continue;
+        }
+        if (!overlaps(qlo, qhi, qlo_of(x), qhi_of(x))) continue;
+        if (x >= n - 1) {
+          int j = (int)vals[x - (n - 1)];
+          if (keep(i, j)) emit(j);
+        } else if (sp < kStack) {
+          stack[sp++] = x;
+        } else {
+          raise_status(status, XPBD_ERR_OVERFLOW);
+        }
+      }
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+  };
+  // Every warp runs the same iterations (bodies past a group's range are
+  // no-ops), so all 32 lanes meet at each shuffle; sums and scans stay within
+  // each 8-lane segment.
+  const int l = tid & 7, G = tid >> 3, NG = T >> 3;
+  const unsigned full = 0xffffffffu;
+  const int lead = (tid & 31) & ~7;
+  // lane l's subtree: three levels down from the root along the bits of l
+  // (most significant first); a lane whose path reaches a leaf early owns it
+  // only if its remaining bits are zero, so the subtrees are disjoint and
+  // cover every leaf
+  int my_start = 0;
+  for (int d = 0; d < kFrontierRounds && my_start >= 0; ++d) {
+    const int bit = (l >> (kFrontierRounds - 1 - d)) & 1;
+    if (my_start < n - 1) {
+      int2 c = child[my_start];
+      my_start = bit ? c.y : c.x;
+    } else if (bit) {
+      my_start = -1;
+    }
+  }
+  auto count_body = [&](int i) {
+    int c = 0;
+    query_from(i, my_start, [&](int) { ++c; });
+    return c;
+  };
+  // bodies interleaved over the cluster (i = rank + csize k), so the dense
+  // parts of a scene spread over every CTA; the k-th body of this CTA goes to
+  // group k mod NG
+  const int mine_n = n > (int)rank ? (n - (int)rank + (int)csize - 1) / (int)csize : 0;
+  const int gper = (mine_n + NG - 1) / NG;  // the same for every group of the CTA
+  auto body_of = [&](int k) { return (int)rank + (int)csize * (G + NG * k); };
+  int saved[kMaxGroupBodies];  // this lane's count per body (registers: the loop is unrolled)
+#pragma unroll
+  for (int k = 0; k < kMaxGroupBodies; ++k) {
+    saved[k] = 0;
+    if (k < gper) {
+      const int i = body_of(k);
+      int c = i < n ? count_body(i) : 0;
+      saved[k] = c;
+      c += __shfl_xor_sync(full, c, 4);
+      c += __shfl_xor_sync(full, c, 2);
+      c += __shfl_xor_sync(full, c, 1);
+      if (i < n && l == 0) counts[i] = c;
+    }
+  }
+  cluster_sync_all();  // every body's count is in global memory (cluster-scope release/acquire)
+  // per-body offsets: every CTA scans all n counts (two consecutive bodies per thread)
+  int* offs = flags;  // the refit flags are dead
+  int total = 0;
+  {
+    const int b0 = 2 * tid, b1 = b0 + 1;
+    const int v0 = b0 < n ? counts[b0] : 0, v1 = b1 < n ? counts[b1] : 0;
+    int ex = block_exclusive_scan(v0 + v1, s_scan, &total);
+    if (b0 < n) offs[b0] = ex;
+    if (b1 < n) offs[b1] = ex + v0;
+    for (int b = 2 * T + tid; b < n; b += T) offs[b] = 0;  // n <= 2 T always holds here
+  }
+  __syncthreads();
+  if (rank == 0 && tid == 0) {
+    *s.n_pairs = total;
+    if (total > s.cap) raise_status(status, XPBD_ERR_OVERFLOW);
+  }
+  int* stage = stage_all + G * kStagePairs;
+#pragma unroll
+  for (int k = 0; k < kMaxGroupBodies; ++k) {
+    if (k < gper) {
+      const int i = body_of(k);
+      const bool live = i < n;
+      const int c = saved[k];
+      int ex = c;  // exclusive prefix of the lane counts within the group
+      for (int o = 1; o < 8; o <<= 1) {
+        int y = __shfl_up_sync(full, ex, o, 8);
+        if (l >= o) ex += y;
+      }
+      const int body_total = __shfl_sync(full, ex, lead + 7);
+      ex -= c;
+      const int base = live ? offs[i] : 0;
+      const bool staged = body_total <= kStagePairs;
+      if (live && c > 0) {
+        int r = 0;
+        query_from(i, my_start, [&](int j) {
+          if (staged) stage[ex + r] = j;
+          else if (base + ex + r < s.cap) s.pairs[base + ex + r] = make_int2(i, j);
+          ++r;
+        });
+      }
+      __syncwarp();
+      if (live && l == 0) {
+        if (staged) {  // insertion sort by j in shared memory (the partners are distinct)
+          for (int a = 1; a < body_total; ++a) {
+            int key = stage[a], b2 = a - 1;
+            while (b2 >= 0 && stage[b2] > key) {
+              stage[b2 + 1] = stage[b2];
+              --b2;
+            }
+            stage[b2 + 1] = key;
+          }
+        } else {
+          sort_segment(s.pairs, base, min(base + body_total, s.cap));
+        }
+      }
+      __syncwarp();
+      if (live && staged)
+        for (int q = l; q < body_total; q += 8)
+          if (base + q < s.cap) s.pairs[base + q] = make_int2(i, stage[q]);
+      __syncwarp();
+    }
+  }
+}
+
+// =================================================================================
 // Hash-grid broad phase (kernels_hashgrid.py:122-173 over wp.HashGrid): for body
 // i, the bodies whose cell floor(x/cell) lies in floor((x_i -+ qr)/cell) on
 // every axis, j > i, passing the per-axis inflated-box test.
@@ -1972,8 +2295,46 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
   int per_sm = 0;
   XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, substep_kernel(h), h->threads, 0));
   per_sm = std::max(per_sm, 1);
-  int want = std::max(1, ceil_div(work, h->threads));
+  // one thread per item, or one eight-lane group per item
+  int want = std::max(1, ceil_div(h->lanes == 8 ? 8 * work : work, h->threads));
   h->blocks = std::min(h->force_blocks > 0 ? h->force_blocks : want, per_sm * num_sms());
+  return XPBD_OK;
+}
+
+// Cluster size of the fused LBVH broad phase on the current device (largest of
+// 16, 8, 4, 2, 1 CTAs with the maximum shared memory that can be co-scheduled;
+// 0 = the fused path cannot run), chosen once per device.
+static int bp_fused_cluster_size(int* out) {
+  static int chosen[64];
+  static bool done[64] = {false};
+  int dev = 0;
+  XPBD_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return XPBD_ERR_BAD_ARG;
+  if (!done[dev]) {
+    const size_t smem = bp_fused_smem(kFusedMaxBoxes);
+    XPBD_CUDA(cudaFuncSetAttribute(k6_bp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    XPBD_CUDA(cudaFuncSetAttribute(k6_bp_fused, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    int pick = 0;
+    for (int c = 16; c >= 1 && !pick; c /= 2) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(c);
+      cfg.blockDim = dim3(1024);
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = c;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int nc = 0;
+      if (cudaOccupancyMaxActiveClusters(&nc, k6_bp_fused, &cfg) == cudaSuccess && nc > 0) pick = c;
+      cudaGetLastError();
+    }
+    chosen[dev] = pick;
+    done[dev] = true;
+  }
+  *out = chosen[dev];
   return XPBD_OK;
 }
 
@@ -1988,6 +2349,26 @@ static int run_broadphase(xpbd6_solver* h, cudaStream_t st) {
   }
   const int blocks = stream_blocks(n, 256);
   int rc;
+  if (h->par.broadphase == 0 && !s.scene && n <= kFusedMaxBoxes) {
+    int csize = 0;
+    if ((rc = bp_fused_cluster_size(&csize))) return rc;
+    if (csize > 0) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(csize);
+      cfg.blockDim = dim3(1024);
+      cfg.dynamicSmemBytes = bp_fused_smem(n);
+      cfg.stream = st;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = csize;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      XPBD_CUDA(cudaLaunchKernelEx(&cfg, k6_bp_fused, s, h->p6, b.counts, status));
+      return XPBD_OK;
+    }
+  }
   if (h->par.broadphase == 0) {
     k6_bp_init<<<1, 32, 0, st>>>(b);
     if (s.scene) XPBD_CUDA(cudaMemsetAsync(b.roots, 0xff, sizeof(int) * (size_t)s.n_scenes, st));
