@@ -74,6 +74,7 @@ def tune6(s, frames=3, candidates=None):
         best = _CACHE[key][0]
         s.lanes = best[3] if len(best) > 3 else 8
         s.set_driver(*best[:3])
+        s._bind()  # bind now: callers may drive the handle directly, without step()
         return _CACHE[key][1]
     if candidates is None:
         candidates = [(2, 16, 512, 8), (2, 16, 256, 8), (2, 8, 512, 8), (0, 0, 256, 8), (0, 0, 512, 8),
@@ -103,6 +104,7 @@ def tune6(s, frames=3, candidates=None):
     best = results[best_tag][1]
     s.lanes = best[3] if len(best) > 3 else 8
     s.set_driver(*best[:3])
+    s._bind()  # bind now: callers may drive the handle directly, without step()
     report = {"chosen": {"mode": best_tag[0], "blocks": best_tag[1], "threads": best_tag[2], "lanes": best_tag[3]},
               "ms_per_frame": {f"{t[0]}x{t[1]}x{t[2]}x{t[3]}": round(v[0], 5) for t, v in results.items()}}
     _CACHE[key] = (best, report)
