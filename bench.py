@@ -196,7 +196,9 @@ def time_batch(args, device, flush_buf, clocks=None, n_scenes=256, sample=(0, 1,
     alg6 = S * (I * (pts * 196 + 8 * n6 * 47) + npairs * 300 + n6 * 128)
     return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=frame_ms, proj_per_frame=proj,
                 rows=rows3, bodies=n3 + n6, status=b.piles.status() | b.cloth.status(), alg_bytes=alg3 + alg6,
-                launches=args.steps * 17,
+                # cloth frame 1 + piles: multi-kernel LBVH (init, aabb, morton, sort, build,
+                # refit, count, scan (3), write) + substeps 1
+                launches=args.steps * 13,
                 launch={"cloth": b.cloth.launch_info(), "piles": b.piles.launch_info(), "autotune": tune,
                         "build_s": round(build_s, 1), "residual_max": float(res.max()),
                         "residual_median": float(np.median(res)), "vs_solo": checks,
@@ -223,7 +225,10 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
     L = N.lib()
     stream = torch.cuda.current_stream(device)
     sp = C.c_void_p(stream.cuda_stream)
-    launches_per_frame = 1 + (10 if s._self_collision else 0)
+    # frame kernel + contact build: one fused cluster launch up to 4096 collidable
+    # spheres, else init, sanitize, cells, keys, sort, count, scan (3), write
+    n_coll = int(s.tensors["collide_idx"].numel()) if s._self_collision else 0
+    launches_per_frame = 1 + ((1 if n_coll <= 4096 else 10) if s._self_collision else 0)
 
     def frame():
         if s._self_collision:
@@ -330,7 +335,8 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
     S, I = s.substeps, s.iterations
     alg = S * (I * (points * 196 + 8 * n_dyn * 47 + s.num_joints * 196) + npairs * 300 + n * 128)
     return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=kern_ms, proj_per_frame=proj_per_frame,
-                rows=rows, bodies=n, status=status, alg_bytes=alg, launches=args.steps * 16, solver=s,
+                rows=rows, bodies=n, status=status, alg_bytes=alg, launches=args.steps * 2, solver=s,
+                kernel="k6_substeps8" if s.lanes == 8 else "k6_substeps",
                 launch=dict(s.launch_info(), pairs=npairs, manifold_points=points,
                             graph_ms_per_frame=round(graph_ms, 5), autotune=tune["ms_per_frame"]))
 
@@ -515,8 +521,8 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 5), "peak_kind": peak_kind,
                          "traffic": traffic_for(args.workload),
-                         "kernel": {"batch": "k3_frames + k6_substeps (whole frame)"}.get(
-                             args.workload, "k6_substeps" if args.workload in SIX_DOF else "k3_frames"),
+                         "kernel": r.get("kernel", {"batch": "k3_frames + k6_substeps (whole frame)"}.get(
+                             args.workload, "k3_frames")),
                          "kernel_ms": round(kern_ms, 5), "alg_bytes_per_launch": r["alg_bytes"]},
             "gpu_launches": r["launches"],
             "status_bits": r["status"],
