@@ -66,6 +66,40 @@ def test_frames_match_oracle(golden, name, build, frames, lanes):
         assert np.abs(eng.omega.numpy() - orc.omega).max() <= 9000 * tol
 
 
+@pytest.mark.parametrize("lanes", [8, 1])
+@pytest.mark.parametrize("name", ["pile_lbvh", "stack", "joints"])
+def test_one_substep_positions_and_lambdas(golden, name, lanes):
+    """One substep at a time on identical state (the oracle re-seeded from the
+    engine before each): positions within 1e-5 m, orientations within 1e-5, and
+    the floor, manifold and joint multipliers within 1e-4 of the largest
+    multiplier of their kind."""
+    build = dict((f[0], f[1]) for f in fixtures6())[name]
+    kw = kwargs(golden(name))
+    kw["dt"] = kw.get("dt", 1 / 60) / kw["substeps"]
+    kw["substeps"] = 1
+    eng, orc = _pair(build, **kw)
+    eng.lanes = lanes
+    for k in range(8):
+        if k:
+            _reseed_oracle(orc, eng)
+        eng.step()
+        orc.step()
+        n_pairs = orc.n_pairs
+        assert eng.n_pairs == n_pairs
+        np.testing.assert_array_equal(eng.pairs(), np.stack([orc.pair_a[:n_pairs], orc.pair_b[:n_pairs]], 1))
+        assert np.abs(eng.positions() - orc.positions()).max() <= 1e-5
+        assert np.abs(eng.orientations() - orc.orientations()).max() <= 1e-5
+        T = eng.tensors
+        n = eng.num_bodies
+        for got, want in ((T["lam_floor"][: 8 * n], orc.lam_floor[: 8 * n]),
+                          (T["lam_pair"][: 8 * n_pairs], orc.lam_pair[: 8 * n_pairs]),
+                          (T["lam_joint"][: eng.num_joints], orc.lam_joint[: eng.num_joints])):
+            got = got.cpu().numpy()
+            if want.size:
+                scale = max(float(np.abs(want).max()), 1e-12)
+                assert np.abs(got - want).max() <= 1e-4 * scale, (k, np.abs(got - want).max(), scale)
+
+
 @pytest.mark.parametrize("bp", ["lbvh", "hashgrid", "grid"])
 def test_pairs_1440_bit_exact(golden, bp):
     g = golden(f"pairs1440_{bp}")
