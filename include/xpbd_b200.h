@@ -226,6 +226,8 @@ typedef struct xpbd6_params {
     float floor_y, friction, restitution, lin_damp, ang_damp, jacobi_relax;
     float max_speed, max_omega, man_margin;
     int broadphase;  /* 0 lbvh, 1 hashgrid, 2 grid */
+    int edge_axes;   /* 1: the manifold also tests the nine edge-edge SAT axes (no reference
+                        counterpart: kernels_6dof.py:13-15 tests face axes only); 0: as the reference */
 } xpbd6_params;
 
 /* kernels_6dof.py:68-102 integrate_bodies */

@@ -59,7 +59,7 @@ class xpbd6_params(C.Structure):
                 ("floor_y", C.c_float), ("friction", C.c_float), ("restitution", C.c_float),
                 ("lin_damp", C.c_float), ("ang_damp", C.c_float), ("jacobi_relax", C.c_float),
                 ("max_speed", C.c_float), ("max_omega", C.c_float), ("man_margin", C.c_float),
-                ("broadphase", C.c_int)]
+                ("broadphase", C.c_int), ("edge_axes", C.c_int)]
 
 
 _SIGS = {

@@ -44,6 +44,7 @@ struct Dev6 {
 struct Par6 {
   float h, dt, gx, gy, gz, floor_y, mu, rest, lin_damp, ang_damp, relax, max_speed, max_omega, margin;
   int substeps, iterations, gyro;
+  int edge_axes;  // 1: also the nine edge-edge SAT axes (off: the reference's face-only manifold)
 };
 
 XD void vadd(float4* p, V3 d, float c) { red_add4(p, make_float4(d.x, d.y, d.z, c)); }
@@ -133,7 +134,70 @@ XD float proj_radius(V3 L, const M33& R, V3 e) {
   return fabsf(e.x * dot(L, mcol(R, 0))) + fabsf(e.y * dot(L, mcol(R, 1))) + fabsf(e.z * dot(L, mcol(R, 2)));
 }
 
-XD void manifold_pair(const Dev6& s, int pid, float margin) {
+// Edge-edge SAT axes (no reference counterpart: the reference tests the six face
+// axes only, kernels_6dof.py:13-15, so two boxes whose edges cross can get a
+// face manifold with a tilted normal, or a contact while an edge axis separates
+// them).  Called after the face axes found no separation, with their smallest
+// overlap.  Returns -1 when an edge axis separates the boxes (the pair gets no
+// manifold), 0 when the face manifold stays (no edge axis is clearly better:
+// below 0.95 x the best face overlap minus 5 mm), 1 after writing a one-point
+// manifold at the closest points of the two supporting edges, incident body a,
+// reference body b, normal from b towards a.
+XD int edge_contact(const Dev6& s, int pid, int a, int b, V3 cA, V3 cB, V3 eA, V3 eB, const M33& RA,
+                    const M33& RB, float face_best, float margin) {
+  const V3 d = cA - cB;
+  float best = 1.0e30f;
+  int bi = -1, bj = -1;
+  V3 bestL = V3{0.0f, 1.0f, 0.0f};
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) {
+      V3 L = cross(mcol(RA, i), mcol(RB, j));
+      float len = length(L);
+      if (len < 1.0e-5f) continue;  // parallel edges: the face axes cover them
+      L = L / len;
+      float ov = proj_radius(L, RA, eA) + proj_radius(L, RB, eB) - fabsf(dot(L, d));
+      if (ov < 0.0f) return -1;
+      if (ov < best) {
+        best = ov;
+        bi = i;
+        bj = j;
+        bestL = L;
+      }
+    }
+  }
+  if (bi < 0 || !(best < 0.95f * face_best - 0.005f)) return 0;
+  V3 n = bestL;
+  if (dot(n, d) < 0.0f) n = -n;  // from b towards a
+  // supporting edges: a's edge along its axis bi nearest b, b's edge along bj nearest a
+  V3 pa0 = cA, pb0 = cB;
+  for (int k = 0; k < 3; ++k) {
+    if (k != bi) {
+      V3 ak = mcol(RA, k);
+      pa0 = pa0 + ak * (dot(ak, n) > 0.0f ? -comp(eA, k) : comp(eA, k));
+    }
+    if (k != bj) {
+      V3 bk = mcol(RB, k);
+      pb0 = pb0 + bk * (dot(bk, n) > 0.0f ? comp(eB, k) : -comp(eB, k));
+    }
+  }
+  const V3 da = mcol(RA, bi), db = mcol(RB, bj);
+  const V3 w = pa0 - pb0;
+  const float c = dot(da, db), denom = 1.0f - c * c;
+  if (!(denom > 1.0e-6f)) return 0;
+  float sa = (c * dot(db, w) - dot(da, w)) / denom;
+  float tb = (dot(db, w) - c * dot(da, w)) / denom;
+  sa = fminf(fmaxf(sa, -comp(eA, bi)), comp(eA, bi));
+  tb = fminf(fmaxf(tb, -comp(eB, bj)), comp(eB, bj));
+  const V3 pa = pa0 + da * sa, pb = pb0 + db * tb;
+  if (!(dot(pa - pb, n) < margin)) return -1;
+  s.m_off_inc[8 * pid] = f4(mtv(RA, pa - cA), 0.0f);
+  s.m_off_ref[8 * pid] = f4(mtv(RB, pb - cB), 0.0f);
+  s.m_normal[pid] = f4(n, 0.0f);
+  s.m_hdr[pid] = make_int4(1, a, b, 0);
+  return 1;
+}
+
+XD void manifold_pair(const Dev6& s, int pid, float margin, int edge_axes = 0) {
   int4 hdr = make_int4(0, 0, 0, 0);
 #pragma unroll
   for (int c = 0; c < 8; ++c) s.lam_pair[8 * pid + c] = 0.0f;
@@ -156,6 +220,11 @@ XD void manifold_pair(const Dev6& s, int pid, float margin) {
     float ov = comp(eB, k) + proj_radius(L, RA, eA) - fabsf(dot(L, cBA));
     if (ov < 0.0f) { s.m_hdr[pid] = hdr; return; }
     if (ov < best_overlap) { best_overlap = ov; best_axis = L; ref_is_a = 0; best_k = k; }
+  }
+  if (edge_axes) {
+    int r = edge_contact(s, pid, a, b, cA, cB, eA, eB, RA, RB, best_overlap, margin);
+    if (r < 0) { s.m_hdr[pid] = hdr; return; }
+    if (r > 0) return;
   }
   V3 nBA = best_axis;
   if (dot(nBA, cBA) < 0.0f) nBA = -nBA;
@@ -751,7 +820,7 @@ XD void velocity_box8(const Dev6& s, int pid, const Par6& p, const Grp& G) {
 }
 
 // generate_box_manifold with 8 lanes; `stage` is this group's 8-vertex buffer.
-XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float4* stage) {
+XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float4* stage, int edge_axes = 0) {
   s.lam_pair[8 * pid + G.l] = 0.0f;
   int2 pr = s.pairs[pid];
   const int a = pr.x, b = pr.y;
@@ -781,6 +850,15 @@ XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float
       ov = ov2;
       bi = b2;
     }
+  }
+  if (edge_axes) {  // one lane runs the edge test (the same arithmetic as the thread-per-pair path)
+    int r = 0;
+    if (G.l == 0) {
+      r = edge_contact(s, pid, a, b, cA, cB, eA, eB, RA, RB, ov, margin);
+      if (r < 0) s.m_hdr[pid] = make_int4(0, 0, 0, 0);
+    }
+    r = __shfl_sync(G.mask, r, G.base);
+    if (r != 0) return;
   }
   V3 best_axis = V3{0.0f, 1.0f, 0.0f};
   int ref_is_a = 1, best_k = 0;
@@ -888,7 +966,7 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
   grid_sync(bar);
   for (int sub = 0; sub < p.substeps; ++sub) {
     const bool more = sub + 1 < p.substeps;
-    for (int pid = t0; pid < np; pid += st) manifold_pair(s, pid, p.margin);
+    for (int pid = t0; pid < np; pid += st) manifold_pair(s, pid, p.margin, p.edge_axes);
     grid_sync(bar);
     for (int it = 0; it < p.iterations; ++it) {
       const int work = nj + n + np;
@@ -943,7 +1021,7 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
   grid_sync(bar);
   for (int sub = 0; sub < p.substeps; ++sub) {
     const bool more = sub + 1 < p.substeps;
-    for (int pid = g0; pid < np; pid += gs) manifold_pair8(s, pid, p.margin, G, my_stage);
+    for (int pid = g0; pid < np; pid += gs) manifold_pair8(s, pid, p.margin, G, my_stage, p.edge_axes);
     grid_sync(bar);
     for (int it = 0; it < p.iterations; ++it) {
       for (int t = t0; t < nj; t += st) joint_row(s, t, p.h);
@@ -2045,6 +2123,7 @@ static Par6 make_par6(const xpbd6_params* p) {
   q.substeps = p->substeps;
   q.iterations = p->iterations;
   q.gyro = p->gyroscopic;
+  q.edge_axes = p->edge_axes ? 1 : 0;
   return q;
 }
 

@@ -104,7 +104,8 @@ class Solver6DOF:
                  gravity=(0.0, -9.81, 0.0), floor_y: float = 0.0, friction: float = 0.6,
                  restitution: float = 0.0, lin_damp: float = 0.0, ang_damp: float = 0.0,
                  gyroscopic: bool = False, jacobi_relax: float = 1.0, device: str = "cuda:0",
-                 max_speed: float = 60.0, max_omega: float = 60.0, broadphase: str = "lbvh"):
+                 max_speed: float = 60.0, max_omega: float = 60.0, broadphase: str = "lbvh",
+                 edge_axes: bool = False):
         self.device = N.require_cuda(device)
         self.dt = float(dt)
         self.substeps = int(substeps)
@@ -119,6 +120,10 @@ class Solver6DOF:
         self.jacobi_relax = float(jacobi_relax)
         self.max_speed = float(max_speed)
         self.max_omega = float(max_omega)
+        # Not in the reference (kernels_6dof.py:13-15 tests face axes only): also
+        # test the nine edge-edge SAT axes, giving crossing edges a one-point
+        # manifold with the edge-edge normal.  Off by default (reference results).
+        self.edge_axes = bool(edge_axes)
         if broadphase not in BROADPHASES:
             raise ValueError(f"broadphase must be one of {sorted(BROADPHASES)}")
         self.broadphase = str(broadphase)
@@ -303,13 +308,14 @@ class Solver6DOF:
         p.max_omega = self.max_omega
         p.man_margin = self._man_margin
         p.broadphase = BROADPHASES[self.broadphase]
+        p.edge_axes = 1 if self.edge_axes else 0
         return p
 
     def _signature(self):
         """solver_6dof.py:481-487: parameters baked into a bound handle / graph."""
         return (self.cap, self.substeps, self.iterations, self.gyroscopic, self.dt, self.gravity, self.floor_y,
                 self.friction, self.restitution, self.lin_damp, self.ang_damp, self.jacobi_relax, self.max_speed,
-                self.max_omega, self._man_margin, self.broadphase, self.driver, self.lanes)
+                self.max_omega, self._man_margin, self.broadphase, self.driver, self.lanes, self.edge_axes)
 
     def _bind(self):
         L = lib6()
