@@ -58,6 +58,27 @@ def test_frames_match_oracle(golden, name, build, frames):
         assert eng.num_colors == orc.num_colors
 
 
+@pytest.mark.parametrize("drv", [(2, 4, 256), (0, 0, 256)], ids=["cluster", "grid"])
+@pytest.mark.parametrize("name", ["cloth6_jacobi", "spheres18_jacobi", "chain_jacobi"])
+def test_folded_jacobi_drivers_match_oracle(golden, name, drv):
+    """The cluster and grid drivers fold each Jacobi apply into the next
+    iteration's position reads (one barrier per iteration instead of two); the
+    frames still follow the oracle to float-atomic rounding, multipliers too."""
+    build, frames = dict((f[0], (f[1], f[2])) for f in fixtures3())[name]
+    kw = kwargs(golden(name))
+    eng, orc = _pair(build, **kw)
+    eng.set_driver(*drv)
+    for f in range(frames):
+        eng.step()
+        orc.step()
+        assert eng.status() == 0
+        assert eng.launch_info()["mode"] == ("cluster" if drv[0] == 2 else "grid")
+        dx = np.abs(eng.positions() - orc.positions()).max()
+        assert dx <= 1e-5 * (f + 1) ** 2, f"frame {f}: max|dx| {dx}"
+        if f == 0:
+            assert _lam_close(eng.lambdas(), orc.lambdas()), np.abs(eng.lambdas() - orc.lambdas()).max()
+
+
 @pytest.mark.parametrize("mode", ["gs", "jacobi"])
 def test_one_substep_cloth32(mode):
     """One substep of the 32 x 32 cloth: x within 1e-5 m, lambda within 1e-4 rel."""

@@ -36,11 +36,14 @@ struct Dev3 {
   const int* cstarts;
   int n;
   int ncolors;
+  float4* accs = nullptr;  // folded Jacobi: one accumulator per iteration (handle memory)
+  int acc_stride = 0;
 };
 
 struct Par3 {
   float h, gx, gy, gz, damping, relax, max_speed;
   int cap_on, substeps, iterations, gs;
+  int fold = 0;  // 1: Jacobi with the apply folded into the next iteration's reads
 };
 
 // ---------------------------------------------------------------------------
@@ -93,10 +96,35 @@ XD void body_finalize(const float4* x, const float4* xp, float4* v, int i, float
   v[i] = f4(vi, 0.0f);
 }
 
+// Particle positions as the row projection reads them: straight from x, or
+// x with the averaged corrections of the earlier iterations of this substep
+// applied on the fly (the folded driver: the corrections of iteration m sit in
+// acc + m * stride; the expression is apply_jacobi's, kernels.py:326-339).
+struct PosPlain {
+  const float4* x;
+  XD float4 operator[](int i) const { return x[i]; }
+};
+struct PosFolded {
+  const float4* x;
+  const float4* acc;
+  size_t stride;
+  int n_prev;
+  float relax;
+  XD float4 operator[](int i) const {
+    float4 xi = x[i];
+    for (int m = 0; m < n_prev; ++m) {
+      float4 a = acc[m * stride + i];
+      int c = (int)a.w;
+      if (c > 0 && xi.w > 0.0f) xi = f4(v3(xi) + v3(a) * (relax / (float)c), xi.w);
+    }
+    return xi;
+  }
+};
+
 // kernels.py:219-322 solve_constraints_jacobi, one row.  `acc(i, d)` adds the
-// correction d (and one to the count) to particle i.
-template <bool FIRST, class Acc>
-XD void row_jacobi(const float4* x, const float4* xp, const int4* ri, const float4* rf,
+// correction d (and one to the count) to particle i; `x[i]` reads a position.
+template <bool FIRST, class Acc, class Pos>
+XD void row_jacobi(Pos x, const float4* xp, const int4* ri, const float4* rf,
                    const float4* ra, float* lam, int j, float h, Acc acc) {
   int4 r = ri[j];
   float lam_old = FIRST ? 0.0f : lam[j];
@@ -297,7 +325,7 @@ __global__ void k3_jacobi(Dev3 s, float h) {
   int m = *s.n_rows;
   AccGlobal acc{s.acc};
   for (int j = gtid(); j < m; j += gstride())
-    row_jacobi<FIRST>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, j, h, acc);
+    row_jacobi<FIRST>(PosPlain{s.x}, s.xp, s.ri, s.rf, s.ra, s.lam, j, h, acc);
 }
 __global__ void k3_apply(Dev3 s, float relax) {
   for (int i = gtid(); i < s.n; i += gstride()) body_apply(s.x, s.acc, i, relax);
@@ -373,10 +401,20 @@ __global__ void __launch_bounds__(1024) k3_frames(Dev3 g, Par3 p, int frames, Gr
               }
               sync();
             }
+          } else if (!SMEM && p.fold) {
+            // folded Jacobi: read x plus the earlier iterations' averaged corrections,
+            // accumulate into this iteration's own buffer; no apply phase
+            const PosFolded pos{s.x, g.accs, (size_t)g.acc_stride, it, p.relax};
+            const AccGlobal acc_it{g.accs + (size_t)it * g.acc_stride};
+            for (int j = tid0; j < m; j += stride) {
+              if (it == 0) row_jacobi<true>(pos, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
+              else row_jacobi<false>(pos, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
+            }
+            sync();
           } else {
             for (int j = tid0; j < m; j += stride) {
-              if (it == 0) row_jacobi<true>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
-              else row_jacobi<false>(s.x, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
+              if (it == 0) row_jacobi<true>(PosPlain{s.x}, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
+              else row_jacobi<false>(PosPlain{s.x}, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
             }
             sync();
             if (it + 1 < p.iterations) {
@@ -388,7 +426,20 @@ __global__ void __launch_bounds__(1024) k3_frames(Dev3 g, Par3 p, int frames, Gr
       }
       // last apply (Jacobi) + finalize + clamp + the next substep's integrate, per body
       for (int i = tid0; i < n; i += stride) {
-        if (!GS && m > 0 && p.iterations > 0) body_apply(s.x, s.acc, i, p.relax);
+        if (!GS && !SMEM && p.fold && m > 0 && p.iterations > 0) {
+          // every iteration's averaged correction in order, as apply_jacobi would
+          float4 xi = s.x[i];
+          for (int it = 0; it < p.iterations; ++it) {
+            float4* ap = g.accs + (size_t)it * g.acc_stride + i;
+            float4 a = *ap;
+            *ap = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            int c = (int)a.w;
+            if (c > 0 && xi.w > 0.0f) xi = f4(v3(xi) + v3(a) * (p.relax / (float)c), xi.w);
+          }
+          s.x[i] = xi;
+        } else if (!GS && m > 0 && p.iterations > 0) {
+          body_apply(s.x, s.acc, i, p.relax);
+        }
         body_finalize(s.x, s.xp, s.v, i, p.h, p.damping, p.cap_on, p.max_speed);
         if (more) body_integrate(s.x, s.v, s.xp, i, p.h, gv);
       }
@@ -502,6 +553,8 @@ struct xpbd3_solver {
   size_t smem = 0;
   int mode = 0;
   int force_mode = -1, force_blocks = 0, force_threads = 0;
+  float4* accs = nullptr;  // folded Jacobi accumulators (zero between launches)
+  size_t accs_bytes = 0;
 };
 
 static constexpr size_t kSmemMax = 227 * 1024;
@@ -610,6 +663,7 @@ extern "C" int xpbd3_create(xpbd3_solver** out) {
 extern "C" int xpbd3_destroy(xpbd3_solver* h) {
   if (!h) return XPBD_OK;
   if (h->bar) cudaFree(h->bar);
+  if (h->accs) cudaFree(h->accs);
   delete h;
   return XPBD_OK;
 }
@@ -659,6 +713,25 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   } else {
     h->smem = 0;
     h->threads = h->force_threads > 0 ? h->force_threads : (mode == 2 ? 1024 : 256);
+  }
+  // Jacobi on the cluster / grid drivers with 2-4 iterations: fold each apply
+  // into the next iteration's reads (one barrier per iteration instead of two)
+  q.fold = 0;
+  h->dev.accs = nullptr;
+  h->dev.acc_stride = 0;
+  if (!p->gs && mode != 1 && p->iterations >= 2 && p->iterations <= 4 && s->n_bodies > 0) {
+    size_t bytes = sizeof(float4) * (size_t)s->n_bodies * (size_t)p->iterations;
+    if (bytes > h->accs_bytes) {
+      if (h->accs) cudaFree(h->accs);
+      h->accs = nullptr;
+      h->accs_bytes = 0;
+      XPBD_CUDA(cudaMalloc(&h->accs, bytes));
+      h->accs_bytes = bytes;
+    }
+    XPBD_CUDA(cudaMemset(h->accs, 0, bytes));
+    h->dev.accs = h->accs;
+    h->dev.acc_stride = s->n_bodies;
+    q.fold = 1;
   }
   int rc;
   if (p->gs) rc = mode == 1 ? configure<true, true>(h) : configure<true, false>(h);
