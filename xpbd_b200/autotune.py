@@ -37,7 +37,7 @@ def tune3(s, frames=3, candidates=None):
         s.set_driver(*_CACHE[key][0])
         return _CACHE[key][1]
     if candidates is None:
-        candidates = [(1, 0, 0), (2, 16, 1024), (2, 8, 1024), (2, 4, 1024), (2, 16, 512), (0, 0, 256)]
+        candidates = [(1, 0, 0), (2, 16, 512), (2, 8, 512), (2, 4, 512), (2, 16, 256), (0, 0, 256)]
     stream = torch.cuda.current_stream(s.device)
     sp = C.c_void_p(stream.cuda_stream)
     if s._self_collision:

@@ -351,8 +351,13 @@ __global__ void k3_cap(Dev3 s, float max_speed) {
 // and multipliers in shared memory.  Otherwise the state stays in global
 // memory (L2-resident for these sizes) and phases are separated by the
 // bounded grid barrier of a cooperative launch.
+constexpr int kCachedRows = 1;
+
+// The one-CTA shared-memory driver runs up to 1024 threads; the cluster and
+// grid drivers at most 512 (their best shapes), which leaves room for the
+// registers of the cached rows.
 template <bool GS, bool SMEM>
-__global__ void __launch_bounds__(1024) k3_frames(Dev3 g, Par3 p, int frames, GridBarrier bar) {
+__global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p, int frames, GridBarrier bar) {
   extern __shared__ float4 smem[];
   const int n = g.n;
   const int m = *g.n_rows;
@@ -384,6 +389,25 @@ __global__ void __launch_bounds__(1024) k3_frames(Dev3 g, Par3 p, int frames, Gr
   if (m > 0 && p.iterations == 0) {
     for (int j = tid0; j < m; j += stride) s.lam[j] = 0.0f;
   }
+  // Folded driver with at most kCachedRows rows per thread: the rows (fixed for
+  // the launch) and their multipliers stay in registers; the multipliers are
+  // written back at the end of the launch.
+  const bool cache_rows = !GS && !SMEM && p.fold && m <= kCachedRows * stride;
+  int4 c_ri[kCachedRows];
+  float4 c_rf[kCachedRows];
+  float c_lam[kCachedRows];
+#pragma unroll
+  for (int k = 0; k < kCachedRows; ++k) {
+    const int j = tid0 + k * stride;
+    c_ri[k] = make_int4(0, 0, 0, 0);
+    c_rf[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    c_lam[k] = 0.0f;
+    if (cache_rows && j < m) {
+      c_ri[k] = s.ri[j];
+      c_rf[k] = s.rf[j];
+      c_lam[k] = s.lam[j];
+    }
+  }
   for (int f = 0; f < frames; ++f) {
     for (int i = tid0; i < n; i += stride) body_integrate(s.x, s.v, s.xp, i, p.h, gv);
     sync();
@@ -406,9 +430,20 @@ __global__ void __launch_bounds__(1024) k3_frames(Dev3 g, Par3 p, int frames, Gr
             // accumulate into this iteration's own buffer; no apply phase
             const PosFolded pos{s.x, g.accs, (size_t)g.acc_stride, it, p.relax};
             const AccGlobal acc_it{g.accs + (size_t)it * g.acc_stride};
-            for (int j = tid0; j < m; j += stride) {
-              if (it == 0) row_jacobi<true>(pos, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
-              else row_jacobi<false>(pos, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
+            if (cache_rows) {
+#pragma unroll
+              for (int k = 0; k < kCachedRows; ++k) {
+                const int j = tid0 + k * stride;
+                if (j < m) {
+                  if (it == 0) row_jacobi<true>(pos, s.xp, &c_ri[k], &c_rf[k], s.ra + j, &c_lam[k], 0, p.h, acc_it);
+                  else row_jacobi<false>(pos, s.xp, &c_ri[k], &c_rf[k], s.ra + j, &c_lam[k], 0, p.h, acc_it);
+                }
+              }
+            } else {
+              for (int j = tid0; j < m; j += stride) {
+                if (it == 0) row_jacobi<true>(pos, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
+                else row_jacobi<false>(pos, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
+              }
             }
             sync();
           } else {
@@ -453,6 +488,13 @@ __global__ void __launch_bounds__(1024) k3_frames(Dev3 g, Par3 p, int frames, Gr
       g.xp[i] = s.xp[i];
     }
     for (int j = threadIdx.x; j < m; j += blockDim.x) g.lam[j] = s.lam[j];
+  }
+  if (cache_rows && p.iterations > 0) {
+#pragma unroll
+    for (int k = 0; k < kCachedRows; ++k) {
+      const int j = tid0 + k * stride;
+      if (j < m) g.lam[j] = c_lam[k];
+    }
   }
 }
 
@@ -712,7 +754,7 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
                                       : (int)std::min<long long>(1024, std::max<long long>(128, ((w + 31) / 32) * 32));
   } else {
     h->smem = 0;
-    h->threads = h->force_threads > 0 ? h->force_threads : (mode == 2 ? 1024 : 256);
+    h->threads = h->force_threads > 0 ? std::min(h->force_threads, 512) : (mode == 2 ? 512 : 256);
   }
   // Jacobi on the cluster / grid drivers with 2-4 iterations: fold each apply
   // into the next iteration's reads (one barrier per iteration instead of two)
