@@ -238,7 +238,7 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
     s._flush()
     for _ in range(args.warmup):
         frame()
-    tune = s.autotune(frames=3)  # on the warmed-up state (contacts present), restored afterwards
+    tune = pin_or_tune(s, args)
     torch.cuda.synchronize(device)
     if world > 1:
         import torch.distributed as dist
@@ -296,7 +296,7 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
     sp = N.stream_of(device)
     for _ in range(SETTLE.get(workload, 0) + args.warmup):
         N.check(L.xpbd6_step(s._h, 1, sp))
-    tune = s.autotune(frames=3)  # on the warmed-up state (contacts present), restored afterwards
+    tune = pin_or_tune(s, args)
     torch.cuda.synchronize(device)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -430,6 +430,21 @@ class _Null:
         return False
 
 
+def pin_or_tune(s, args):
+    """The frame driver for the timed loop: the autotuner on the warmed-up state
+    (contacts present; the state is restored afterwards), or the launch given by
+    --driver MODE,BLOCKS,THREADS[,LANES] (a profiler's timing would mislead the
+    autotuner, so profiles pin the launch the plain run chose)."""
+    if not args.driver:
+        return s.autotune(frames=3)
+    v = [int(t) for t in args.driver.split(",")]
+    if len(v) == 4:
+        s.lanes = v[3]
+    s.set_driver(*v[:3])
+    s._bind()
+    return {"ms_per_frame": {}, "pinned": args.driver}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -475,6 +490,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--driver", default="",
+                    help="pin the frame driver MODE,BLOCKS,THREADS[,LANES] instead of autotuning "
+                         "(mode 0 grid, 1 shared, 2 cluster; LANES 1 or 8 for boxes)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the device-timed loop (for profiler launch lists): no e2e, CPU baseline or extras")
     args = ap.parse_args()

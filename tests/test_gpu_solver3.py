@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 from oracle import oracle as O  # noqa: E402
 from golden_scenes import fixtures3, kwargs  # noqa: E402
 from xpbd_b200 import Solver, scenes  # noqa: E402
+from xpbd_b200.scene import Body  # noqa: E402
 from xpbd_b200 import _native as N  # noqa: E402
 
 
@@ -266,3 +267,35 @@ def test_primitives_sort_and_scan():
         N.check(L.xpbd_scan_i32(N.ptr(ta), N.ptr(out), n, N.ptr(tot), N.stream_of("cuda:0")))
         np.testing.assert_array_equal(out.cpu().numpy(), np.concatenate([[0], np.cumsum(a)[:-1]]))
         assert int(tot.item()) == int(a.sum())
+
+
+def test_setters_edit_in_place_without_rebinding():
+    """Setters write the device tensors in place: no re-bind (and so no graph
+    re-capture) between frames; the edits take effect in the next frame."""
+    twins = []
+    for kick in (False, True):
+        s = Solver(device="cuda:0", dt=1 / 60, substeps=10, iterations=2, solve_mode="jacobi")
+        scenes.build_cloth(s, res=8, spacing=0.05, y=1.0)
+        s.step()
+        binds = s.binds
+        if kick:
+            s.set_velocity(Body(index=5), (0.0, 3.0, 0.0))
+            s.set_all_compliance(1e-4)
+            s.set_all_friction(0.2)
+        s.step()
+        assert s.binds == binds
+        twins.append(s)
+    assert twins[1].positions()[5, 1] > twins[0].positions()[5, 1] + 0.01  # the kick moved body 5 up
+    r = twins[1].rows()
+    assert np.all(r["compliance"][r["type"] == 0] == np.float32(1e-4))
+    assert np.all(r["mu"][r["type"] == 2] == np.float32(0.2))  # FLOOR rows
+
+
+def test_dlpack_export_is_the_live_state():
+    s = Solver(device="cuda:0", dt=1 / 60, substeps=5, iterations=1, solve_mode="jacobi")
+    scenes.build_cloth(s, res=6, spacing=0.05, y=1.0)
+    s.step()
+    x = torch.utils.dlpack.from_dlpack(s.dlpack("x"))
+    np.testing.assert_array_equal(x[:, :3].cpu().numpy(), s.positions())
+    s.step()
+    np.testing.assert_array_equal(x[:, :3].cpu().numpy(), s.positions())  # zero copy: same memory

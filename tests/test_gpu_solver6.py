@@ -265,3 +265,32 @@ def test_kernel_entry_points_match_oracle(golden, entry):
         k = g["m_count"][p]
         np.testing.assert_array_equal(oi[8 * p:8 * p + k], g["m_off_inc"][8 * p:8 * p + k])
         np.testing.assert_array_equal(orf[8 * p:8 * p + k], g["m_off_ref"][8 * p:8 * p + k])
+
+
+def test_setters_edit_in_place_without_rebinding():
+    """set_velocity / add_impulse / set_omega write the device tensors in place:
+    no re-bind (no graph re-capture) between frames, and the edit shows in the
+    next frame."""
+    s = Solver6DOF(device="cuda:0", substeps=10, iterations=2, gravity=(0.0, 0.0, 0.0))
+    s.add_box((0.0, 2.0, 0.0), (0.5, 0.5, 0.5), 1.0)
+    s.add_box((3.0, 2.0, 0.0), (0.5, 0.5, 0.5), 1.0)
+    s.step()
+    binds = s.binds
+    s.set_velocity(0, (0.0, 6.0, 0.0))
+    s.add_impulse(1, (0.0, 0.0, 6.0))
+    s.set_omega(1, (0.0, 2.0, 0.0))
+    s.step()
+    assert s.binds == binds
+    x = s.positions()
+    assert abs(x[0, 1] - 2.1) < 1e-3 and abs(x[1, 2] - 0.1) < 1e-3
+    assert abs(float(s.orientations()[1, 1]) - np.sin(1 / 60)) < 1e-3  # half of 2 rad/s x 1/60 s
+
+
+def test_dlpack_export_is_the_live_state():
+    s = Solver6DOF(device="cuda:0", substeps=5, iterations=1)
+    s.add_box((0.0, 2.0, 0.0), (0.5, 0.5, 0.5), 1.0)
+    s.step()
+    x = torch.utils.dlpack.from_dlpack(s.dlpack("x"))
+    np.testing.assert_array_equal(x[:, :3].cpu().numpy(), s.positions())
+    s.step()
+    np.testing.assert_array_equal(x[:, :3].cpu().numpy(), s.positions())

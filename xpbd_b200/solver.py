@@ -329,6 +329,7 @@ class Solver:
         return tune3(self, frames, candidates)
 
     def _bind(self) -> None:
+        self.binds = getattr(self, "binds", 0) + 1  # handle (re)binds: each one re-captures the frame graph
         L = N.lib()
         if self._h is None:
             h = C.c_void_p()
@@ -440,6 +441,14 @@ class Solver:
         if per_row:
             return res, rows[: int(self._t["n_rows"].item())].cpu().numpy()
         return res
+
+    def dlpack(self, name: str = "x"):
+        """Zero-copy DLPack capsule of one device state tensor (``x``, ``v``, ...,
+        see ``tensors``): headless consumers (a viewer, a renderer, another
+        framework) read the live state without a host copy.  Float4 records:
+        xyz plus the fourth lane of the layout."""
+        self._flush()
+        return torch.utils.dlpack.to_dlpack(self._t[name])
 
     def state_dict(self) -> dict:
         self._flush()

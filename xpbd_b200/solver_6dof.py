@@ -318,6 +318,7 @@ class Solver6DOF:
                 self.max_omega, self._man_margin, self.broadphase, self.driver, self.lanes, self.edge_axes)
 
     def _bind(self):
+        self.binds = getattr(self, "binds", 0) + 1  # handle (re)binds: each one re-captures the frame graph
         L = lib6()
         if self._h is None:
             h = C.c_void_p()
@@ -442,6 +443,14 @@ class Solver6DOF:
         N.check(lib6().xpbd6_residual(C.byref(self._st), C.byref(self._par), N.ptr(body_scene), int(n_scenes),
                                       N.ptr(out), N.stream_of(self.device)), "xpbd6_residual")
         return out.cpu().numpy()
+
+    def dlpack(self, name: str = "x"):
+        """Zero-copy DLPack capsule of one device state tensor (``x``, ``v``, ...,
+        see ``tensors``): headless consumers (a viewer, a renderer, another
+        framework) read the live state without a host copy.  Float4 records:
+        xyz plus the fourth lane of the layout."""
+        self._flush()
+        return torch.utils.dlpack.to_dlpack(self._t[name])
 
     def state_dict(self):
         self._flush()
