@@ -142,6 +142,20 @@ int xpbd3_contacts_build(xpbd3_contacts* c, const xpbd3_state* s, const float* r
                          double contact_margin, double dt, double r_max, int* status_dev,
                          void* stream);
 
+/* solver.py:412-442 Solver.step with self collision, as one CUDA graph per
+ * bind: after this call, xpbd3_step runs per frame the contact rebuild
+ * (xpbd3_contacts_build with these arguments, on the bound state) followed by
+ * the frame kernel, captured once and replayed, with no host work between the
+ * two.  Overflow and reset positions are reported through *status_dev only
+ * (no per-frame host check).  The pointers must stay valid until the next
+ * xpbd3_bind, which detaches, or until a call with c == NULL.  Jacobi only:
+ * Gauss-Seidel colors the contact rows on the host every frame
+ * (XPBD_ERR_BAD_ARG). */
+int xpbd3_attach_contacts(xpbd3_solver* h, xpbd3_contacts* c, const float* radius, const float* friction,
+                          const int* collide_idx, int n_collide, const int64_t* existing, int n_existing,
+                          const float* x_init, double contact_margin, double dt, double r_max,
+                          int* status_dev);
+
 /* No counterpart in the reference.  Same contact rows as xpbd3_contacts_build,
  * for callers that cannot allocate device memory while they step (a plugin
  * whose host owns all GPU allocations, or a fixed-budget simulation thread for

@@ -80,6 +80,44 @@ def test_folded_jacobi_drivers_match_oracle(golden, name, drv):
             assert _lam_close(eng.lambdas(), orc.lambdas()), np.abs(eng.lambdas() - orc.lambdas()).max()
 
 
+def _disjoint_pairs(s):
+    """40 distance pairs over a floor with friction, some partners static: no
+    particle takes more than two corrections per iteration (its pair row and
+    its floor row), so float atomics sum them to the same value in any order."""
+    rng = np.random.default_rng(3)
+    for k in range(40):
+        p = rng.uniform(-1.0, 1.0, 3) * np.array([1.0, 0.0, 1.0]) + np.array([0.0, 0.02 + 0.1 * rng.random(), 0.0])
+        a = s.add_particle(tuple(p), mass=1.0, velocity=tuple(rng.normal(0.0, 2.0, 3)))
+        b = s.add_particle(tuple(p + np.array([0.1, 0.02, 0.0])), mass=0.0 if k % 7 == 0 else 2.0,
+                           velocity=tuple(rng.normal(0.0, 2.0, 3)))
+        s.add_distance(a, b, compliance=1e-6)
+        s.add_floor_contact(a, friction=0.4)
+        s.add_floor_contact(b, friction=0.4)
+
+
+@pytest.mark.parametrize("drv", [(2, 4, 256), (0, 0, 256)], ids=["cluster", "grid"])
+@pytest.mark.parametrize("substeps", [15, 4])
+def test_folded_substeps_bit_exact_on_disjoint_pairs(drv, substeps):
+    """The folded drivers read each substep boundary on the fly (apply, finalize,
+    clamp, integrate inside the first iteration's reads) and store the frame
+    state in one closing pass.  Where atomic order cannot matter they match the
+    oracle bit for bit: positions, velocities, substep-start positions and
+    multipliers, after every frame (odd and even substep counts end in
+    different buffers)."""
+    kw = dict(dt=1 / 60, substeps=substeps, iterations=2, solve_mode="jacobi", damping=0.01, max_speed=3.0)
+    eng, orc = _pair(_disjoint_pairs, **kw)
+    eng.set_driver(*drv)
+    for f in range(4):
+        eng.step()
+        orc.step()
+        assert eng.status() == 0
+        sd = eng.state_dict()
+        np.testing.assert_array_equal(eng.positions(), orc.positions())
+        np.testing.assert_array_equal(eng.velocities(), orc.velocities())
+        np.testing.assert_array_equal(sd["x_prev"][:, :3].cpu().numpy(), orc.x_prev)
+        np.testing.assert_array_equal(eng.lambdas(), orc.lambdas())
+
+
 @pytest.mark.parametrize("mode", ["gs", "jacobi"])
 def test_one_substep_cloth32(mode):
     """One substep of the 32 x 32 cloth: x within 1e-5 m, lambda within 1e-4 rel."""
@@ -299,3 +337,36 @@ def test_dlpack_export_is_the_live_state():
     np.testing.assert_array_equal(x[:, :3].cpu().numpy(), s.positions())
     s.step()
     np.testing.assert_array_equal(x[:, :3].cpu().numpy(), s.positions())  # zero copy: same memory
+
+
+def test_captured_frame_with_contacts_matches_host_driven_frames():
+    """With sync_contacts off, step() attaches the contact rebuild to the handle
+    and replays contact rebuild + frame kernel as one captured graph.  The rows
+    of the first frame are identical to the host-driven path's (same start
+    state), later frames agree to float-atomic rounding, and turning the host
+    check back on detaches."""
+    runs = {}
+    for graph in (False, True):
+        s = Solver(device="cuda:0", dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi")
+        scenes.build_sphere_pile(s, nx=8, ny=4, nz=8, pitch=0.098, y0=0.06, seed=4)
+        s.sync_contacts = not graph
+        s.step()
+        assert s._hooked == graph
+        rows1 = s.rows()
+        for _ in range(3):
+            s.step()
+        assert s.status() == 0
+        runs[graph] = (rows1, s.positions(), s)
+    (ra, xa, _), (rb, xb, sb) = runs[False], runs[True]
+    for k in ("type", "a", "b", "rest", "mu"):
+        np.testing.assert_array_equal(ra[k], rb[k])
+    assert np.abs(xa - xb).max() <= 1e-4
+    sb.sync_contacts = True
+    sb.step()
+    assert not sb._hooked
+    binds = sb.binds
+    sb.sync_contacts = False
+    sb.set_driver(0, 0, 256)  # a re-bind drops the capture; the next step captures the grid driver
+    sb.step()
+    assert sb._hooked and sb.binds == binds + 1 and sb.launch_info()["mode"] == "grid"
+    assert sb.status() == 0

@@ -248,39 +248,66 @@ __global__ void kc_write(ContactArgs a, ContactScratch s) {
 // The rows are identical to the multi-kernel path's.
 constexpr int kFusedMaxCollide = 4096;
 
+// The fused builder's occupied-cell table: open addressing over H = 2^hbits
+// >= 2m slots (linear probing, an empty slot holds kEmptyCell), and per slot
+// its members as a contiguous range of local indices in ascending order --
+// the order a stable sort by cell id gives them (solver.py:514-562), without
+// the sort.
+constexpr uint64_t kEmptyCell = ~0ull;
+
 struct FusedView {
-  uint64_t* skey;  // sorted cid
-  uint32_t* sval;  // sorted local index
-  float4* pos;     // per collidable: sanitized position, radius
+  float4* pos;       // per collidable: sanitized position, radius
+  uint64_t* key;     // [H] cell id of each slot
+  int* start;        // [H + 1] first member of each slot (exclusive scan of the counts)
+  int* member;       // [m] members, slot by slot, ascending within a slot
+  int hbits;
 };
 
+__host__ __device__ inline int fused_hash_bits(int m) {
+  int b = 1;
+  while ((1 << b) < 2 * m) ++b;
+  return b;
+}
+
 static inline size_t fused_smem_bytes(int m) {
-  return (size_t)m * (2 * sizeof(uint64_t) + 2 * sizeof(uint32_t) + sizeof(float4)) +
-         sizeof(unsigned) * (size_t)((14 * m + 31) / 32);
+  const size_t H = (size_t)1 << fused_hash_bits(m);
+  return (size_t)m * sizeof(float4) + H * sizeof(uint64_t) + (H + 1) * sizeof(int) +
+         3 * (size_t)m * sizeof(int) + sizeof(unsigned) * (size_t)((14 * m + 31) / 32);
 }
 
-XD int lower_bound_smem(const uint64_t* s, int m, uint64_t t) {
-  int lo = 0, hi = m;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (s[mid] < t) lo = mid + 1; else hi = mid;
+XD unsigned cell_hash(uint64_t cid, int hbits) {
+  return (unsigned)((cid * 0x9E3779B97F4A7C15ull) >> (64 - hbits));
+}
+
+// Slot of cell `cid`, or -1 when no collidable lies in it.  At most m of the
+// H >= 2m slots are occupied, so a probe meets an empty slot within H steps.
+XD int cell_find(const FusedView& f, uint64_t cid) {
+  const unsigned mask = (1u << f.hbits) - 1u;
+  unsigned h = cell_hash(cid, f.hbits);
+  for (unsigned p = 0; p <= mask; ++p) {
+    const uint64_t k = f.key[h];
+    if (k == cid) return (int)h;
+    if (k == kEmptyCell) return -1;
+    h = (h + 1u) & mask;
   }
-  return lo;
+  return -1;
 }
 
-// visit_slot with the sorted keys and positions read from shared memory.
+// visit_slot over the occupied-cell table in shared memory.
 template <class Emit>
 XD int visit_slot_fused(const ContactArgs& a, const FusedView& f, int o, int k, int64_t cid_k, float margin_f,
                         int64_t S, Emit emit) {
   int64_t delta = ((int64_t)kFwd[o][0] * S + kFwd[o][1]) * S + kFwd[o][2];
   int64_t target = cid_k + delta;
   if (target < 0) return 0;
-  int q = lower_bound_smem(f.skey, a.m, (uint64_t)target);
+  const int h = cell_find(f, (uint64_t)target);
+  if (h < 0) return 0;
   int cnt = 0;
   const int ga = a.coll[k];
   const float4 pa = f.pos[k];
-  for (; q < a.m && f.skey[q] == (uint64_t)target; ++q) {
-    int partner = (int)f.sval[q];
+  const int q1 = f.start[h + 1];
+  for (int q = f.start[h]; q < q1; ++q) {
+    int partner = f.member[q];
     if (o == 0 && !(partner > k)) continue;
     const float4 pb = f.pos[partner];
     float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
@@ -298,22 +325,25 @@ XD int visit_slot_fused(const ContactArgs& a, const FusedView& f, int o, int k, 
   return cnt;
 }
 
-__global__ void __launch_bounds__(1024) kc_fused(ContactArgs a) {
+__global__ void __launch_bounds__(1024, 1) kc_fused(ContactArgs a) {
   extern __shared__ __align__(16) unsigned char fused_dyn[];
-  __shared__ BlockSortSmem sort_sm;
   __shared__ int s_min[3], s_max[3], s_vmax_bits;
   __shared__ int s_warp[32];
   __shared__ int s_cta_total;
+  __shared__ int s_scan[33];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const unsigned rank = cluster_rank(), csize = cluster_size();
   const int m = a.m;
   FusedView f;
-  f.skey = reinterpret_cast<uint64_t*>(fused_dyn);
-  uint64_t* skey2 = f.skey + m;
-  f.pos = reinterpret_cast<float4*>(skey2 + m);
-  f.sval = reinterpret_cast<uint32_t*>(f.pos + m);
-  uint32_t* sval2 = f.sval + m;
-  unsigned* nonempty = sval2 + m;
+  f.hbits = fused_hash_bits(m);
+  const int H = 1 << f.hbits;
+  f.pos = reinterpret_cast<float4*>(fused_dyn);
+  f.key = reinterpret_cast<uint64_t*>(f.pos + m);
+  f.start = reinterpret_cast<int*>(f.key + H);
+  f.member = f.start + H + 1;
+  int* cslot = f.member + m;  // per collidable: its slot
+  int* ticket = cslot + m;    // per collidable: its arrival order in the slot, then its member index
+  unsigned* nonempty = reinterpret_cast<unsigned*>(ticket + m);
   if (tid < 3) {
     s_min[tid] = 0x7fffffff;
     s_max[tid] = (int)0x80000000;
@@ -376,6 +406,10 @@ __global__ void __launch_bounds__(1024) kc_fused(ContactArgs a) {
     }
   }
   for (int i = tid; i < (14 * m + 31) / 32; i += 1024) nonempty[i] = 0u;
+  for (int h = tid; h < H; h += 1024) {
+    f.key[h] = kEmptyCell;
+    f.start[h] = 0;
+  }
   __syncthreads();
   for (int d = 0; d < 3; ++d) {
     red.cmin[d] = s_min[d];
@@ -388,13 +422,52 @@ __global__ void __launch_bounds__(1024) kc_fused(ContactArgs a) {
             cz = (int64_t)(int)floorf(p.z / cell) - red.cmin[2];
     return (cx * S + cy) * S + cz;
   };
-  // 3. keys, 4. stable sort (ties keep ascending index)
+  // 3. cell table: insert every collidable's cell, count its members
   for (int k = tid; k < m; k += 1024) {
-    f.skey[k] = (uint64_t)cid_of(k);
-    f.sval[k] = (uint32_t)k;
+    const uint64_t cid = (uint64_t)cid_of(k);
+    const unsigned mask = (unsigned)H - 1u;
+    unsigned h = cell_hash(cid, f.hbits);
+    for (unsigned p = 0; p <= mask; ++p) {
+      const unsigned long long prev =
+          atomicCAS(reinterpret_cast<unsigned long long*>(f.key + h), (unsigned long long)kEmptyCell,
+                    (unsigned long long)cid);
+      if (prev == kEmptyCell || prev == cid) break;
+      h = (h + 1u) & mask;
+    }
+    cslot[k] = (int)h;
+    ticket[k] = atomicAdd(&f.start[h], 1);
   }
   __syncthreads();
-  block_sort_pairs_u64(sort_sm, f.skey, f.sval, skey2, sval2, m, 63);
+  // 4. slot ranges: exclusive scan of the counts, H / 1024 consecutive slots per thread
+  {
+    const int per = (H + 1023) / 1024;
+    const int h0 = min(tid * per, H), h1 = min(h0 + per, H);
+    int run = 0;
+    for (int h = h0; h < h1; ++h) run += f.start[h];
+    int total = 0;
+    int off = block_exclusive_scan(run, s_scan, &total);
+    for (int h = h0; h < h1; ++h) {
+      const int c = f.start[h];
+      f.start[h] = off;
+      off += c;
+    }
+    if (tid == 0) f.start[H] = total;
+  }
+  __syncthreads();
+  // members in arrival order, then each at its rank among its slot's members
+  // (ascending local index: the stable order)
+  for (int k = tid; k < m; k += 1024) f.member[f.start[cslot[k]] + ticket[k]] = k;
+  __syncthreads();
+  for (int k = tid; k < m; k += 1024) {
+    const int h = cslot[k];
+    const int q0 = f.start[h], q1 = f.start[h + 1];
+    int r = 0;
+    for (int q = q0; q < q1; ++q) r += f.member[q] < k;
+    ticket[k] = q0 + r;
+  }
+  __syncthreads();
+  for (int k = tid; k < m; k += 1024) f.member[ticket[k]] = k;
+  __syncthreads();
   // 5. count this thread's slots (slot t = o m + k) within this CTA's range
   const int slots = 14 * m;
   const int per_cta = (slots + (int)csize - 1) / (int)csize;

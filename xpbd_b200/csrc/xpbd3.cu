@@ -36,14 +36,15 @@ struct Dev3 {
   const int* cstarts;
   int n;
   int ncolors;
-  float4* accs = nullptr;  // folded Jacobi: one accumulator per iteration (handle memory)
+  float4* accs = nullptr;  // folded Jacobi: per-iteration accumulators, then the carry buffers (handle memory)
   int acc_stride = 0;
 };
 
 struct Par3 {
   float h, gx, gy, gz, damping, relax, max_speed;
   int cap_on, substeps, iterations, gs;
-  int fold = 0;  // 1: Jacobi with the apply folded into the next iteration's reads
+  int fold = 0;   // 1: Jacobi with the apply folded into the next iteration's reads
+  int carry = 0;  // 1 (with fold): the substep boundary folded into the first iteration's reads too
 };
 
 // ---------------------------------------------------------------------------
@@ -58,73 +59,145 @@ XD V3 friction_delta(V3 dp_rel, V3 n_hat, float penetration, float mu) {
   return dp_t * (-scale);
 }
 
-// kernels.py:49-73 integrate
+// kernels.py:49-73 integrate, on values: the predicted position; `vi` becomes
+// the integrated velocity (static particles keep both)
+XD float4 integrate_pos(float4 xi, V3& vi, float h, V3 g) {
+  if (xi.w == 0.0f) return xi;
+  vi = vi + g * h;
+  return f4(v3(xi) + vi * h, xi.w);
+}
 XD void body_integrate(float4* x, float4* v, float4* xp, int i, float h, V3 g) {
   float4 xi = x[i];
   xp[i] = make_float4(xi.x, xi.y, xi.z, 0.0f);
   if (xi.w == 0.0f) return;
-  V3 vi = v3(v[i]) + g * h;
+  V3 vi = v3(v[i]);
+  x[i] = integrate_pos(xi, vi, h, g);
   v[i] = f4(vi, 0.0f);
-  x[i] = f4(v3(xi) + vi * h, xi.w);
 }
 
-// kernels.py:326-339 apply_jacobi
+// kernels.py:326-339 apply_jacobi, on values
+XD float4 apply_avg(float4 xi, float4 a, float relax) {
+  int c = (int)a.w;
+  if (c > 0 && xi.w > 0.0f) xi = f4(v3(xi) + v3(a) * (relax / (float)c), xi.w);
+  return xi;
+}
 XD void body_apply(float4* x, float4* acc, int i, float relax) {
   float4 a = acc[i];
-  int c = (int)a.w;
-  if (c > 0) {
-    float4 xi = x[i];
-    if (xi.w > 0.0f) x[i] = f4(v3(xi) + v3(a) * (relax / (float)c), xi.w);
-  }
+  if ((int)a.w > 0) x[i] = apply_avg(x[i], a, relax);
   acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-// kernels.py:346-371 finalize_velocity + cap_velocity
-XD void body_finalize(const float4* x, const float4* xp, float4* v, int i, float h, float damping,
-                      int cap_on, float max_speed) {
-  float4 xi = x[i];
+// kernels.py:346-371 finalize_velocity + cap_velocity, on values
+XD V3 finalize_vel(float4 xi, float4 xpi, float h, float damping, int cap_on, float max_speed) {
   V3 vi;
   if (xi.w == 0.0f) {
     vi = V3{0.0f, 0.0f, 0.0f};
   } else {
-    vi = ((v3(xi) - v3(xp[i])) / h) * (1.0f - damping);
+    vi = ((v3(xi) - v3(xpi)) / h) * (1.0f - damping);
   }
   if (cap_on) {
     float sp = length(vi);
     if (sp > max_speed) vi = vi * (max_speed / sp);
   }
-  v[i] = f4(vi, 0.0f);
+  return vi;
+}
+XD void body_finalize(const float4* x, const float4* xp, float4* v, int i, float h, float damping,
+                      int cap_on, float max_speed) {
+  float4 xi = x[i];
+  float4 xpi = xi.w == 0.0f ? xi : xp[i];
+  v[i] = f4(finalize_vel(xi, xpi, h, damping, cap_on, max_speed), 0.0f);
 }
 
-// Particle positions as the row projection reads them: straight from x, or
-// x with the averaged corrections of the earlier iterations of this substep
-// applied on the fly (the folded driver: the corrections of iteration m sit in
-// acc + m * stride; the expression is apply_jacobi's, kernels.py:326-339).
+// A particle as a row projection reads it: its position (xyz + inverse mass)
+// and, for friction only, its substep-start position.
+struct EndLazy {
+  float4 x;
+  const float4* xp;
+  XD float4 prev() const { return *xp; }
+};
+struct EndHeld {
+  float4 x, p;
+  XD float4 prev() const { return p; }
+};
+
+// Straight from memory.
 struct PosPlain {
   const float4* x;
-  XD float4 operator[](int i) const { return x[i]; }
+  const float4* xp;
+  XD EndLazy operator()(int i) const { return EndLazy{x[i], xp + i}; }
 };
+// The folded drivers run 2..kMaxFoldIters iterations.  A particle's
+// accumulators are loaded together, before any of them is applied, so that
+// their L2 round trips overlap.
+constexpr int kMaxFoldIters = 4;
+XD void load_accs(const float4* acc, size_t stride, int n, int i, float4 (&a)[kMaxFoldIters]) {
+#pragma unroll
+  for (int m = 0; m < kMaxFoldIters; ++m) a[m] = m < n ? acc[m * stride + i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+XD float4 apply_accs(float4 xi, const float4 (&a)[kMaxFoldIters], int n, float relax) {
+#pragma unroll
+  for (int m = 0; m < kMaxFoldIters; ++m)
+    if (m < n) xi = apply_avg(xi, a[m], relax);
+  return xi;
+}
+
+// x with the averaged corrections of the earlier iterations of this substep
+// applied on the fly (folded driver: the corrections of iteration m sit in
+// acc + m * stride).
 struct PosFolded {
   const float4* x;
+  const float4* xp;
   const float4* acc;
   size_t stride;
   int n_prev;
   float relax;
-  XD float4 operator[](int i) const {
+  XD EndLazy operator()(int i) const {
+    float4 a[kMaxFoldIters];
     float4 xi = x[i];
-    for (int m = 0; m < n_prev; ++m) {
-      float4 a = acc[m * stride + i];
-      int c = (int)a.w;
-      if (c > 0 && xi.w > 0.0f) xi = f4(v3(xi) + v3(a) * (relax / (float)c), xi.w);
-    }
-    return xi;
+    load_accs(acc, stride, n_prev, i, a);
+    return EndLazy{apply_accs(xi, a, n_prev, relax), xp + i};
+  }
+};
+// The substep boundary on the fly: the previous substep's predicted position x
+// and start position xp with every iteration's averaged correction applied in
+// order, the velocity finalized and clamped, then integrated into this substep
+// (the expressions of body_apply, body_finalize and body_integrate, in their
+// order, so the values are bit-identical to the unfolded sequence).
+struct PosCarry {
+  const float4* x;
+  const float4* xp;
+  const float4* acc;  // the previous substep's iteration accumulators
+  size_t stride;
+  int iters, cap_on;
+  float relax, h, damping, max_speed;
+  V3 g;
+  XD EndHeld operator()(int i) const {
+    float4 a[kMaxFoldIters];
+    float4 xi = x[i];
+    const float4 xpi = xp[i];
+    load_accs(acc, stride, iters, i, a);
+    xi = apply_accs(xi, a, iters, relax);
+    V3 vi = finalize_vel(xi, xpi, h, damping, cap_on, max_speed);
+    return EndHeld{integrate_pos(xi, vi, h, g), make_float4(xi.x, xi.y, xi.z, 0.0f)};
+  }
+};
+// The frame's first substep on the fly: integrate from the frame-start x, v.
+struct PosStart {
+  const float4* x;
+  const float4* v;
+  float h;
+  V3 g;
+  XD EndHeld operator()(int i) const {
+    const float4 xi = x[i];
+    V3 vi = xi.w == 0.0f ? V3{0.0f, 0.0f, 0.0f} : v3(v[i]);
+    return EndHeld{integrate_pos(xi, vi, h, g), make_float4(xi.x, xi.y, xi.z, 0.0f)};
   }
 };
 
 // kernels.py:219-322 solve_constraints_jacobi, one row.  `acc(i, d)` adds the
-// correction d (and one to the count) to particle i; `x[i]` reads a position.
+// correction d (and one to the count) to particle i; `pos(i)` reads particle i.
 template <bool FIRST, class Acc, class Pos>
-XD void row_jacobi(Pos x, const float4* xp, const int4* ri, const float4* rf,
+XD void row_jacobi(Pos pos, const int4* ri, const float4* rf,
                    const float4* ra, float* lam, int j, float h, Acc acc) {
   int4 r = ri[j];
   float lam_old = FIRST ? 0.0f : lam[j];
@@ -134,14 +207,14 @@ XD void row_jacobi(Pos x, const float4* xp, const int4* ri, const float4* rf,
     if (t == XPBD_DISTANCE || t == XPBD_ATTACH) {
       float inv_dt2 = 1.0f / (h * h);
       int a = r.y;
-      float4 xa = x[a];
+      float4 xa = pos(a).x;
       float wa = xa.w, wb;
       V3 pb;
       if (t == XPBD_ATTACH) {
         pb = v3(ra[j]);
         wb = 0.0f;
       } else {
-        float4 xb = x[r.z];
+        float4 xb = pos(r.z).x;
         pb = v3(xb);
         wb = xb.w;
       }
@@ -162,7 +235,8 @@ XD void row_jacobi(Pos x, const float4* xp, const int4* ri, const float4* rf,
       }
     } else if (t == XPBD_FLOOR) {
       int a = r.y;
-      float4 xa = x[a];
+      const auto ea = pos(a);
+      float4 xa = ea.x;
       float wa = xa.w;
       if (wa != 0.0f) {
         float4 f = rf[j];
@@ -173,7 +247,7 @@ XD void row_jacobi(Pos x, const float4* xp, const int4* ri, const float4* rf,
           V3 corr = V3{0.0f, wa * dlam, 0.0f};
           float mu = f.z;
           if (mu > 0.0f) {
-            V3 dp_rel = (v3(xa) + corr) - v3(xp[a]);
+            V3 dp_rel = (v3(xa) + corr) - v3(ea.prev());
             corr = corr + friction_delta(dp_rel, V3{0.0f, 1.0f, 0.0f}, -C, mu);
           }
           acc(a, corr);
@@ -181,7 +255,9 @@ XD void row_jacobi(Pos x, const float4* xp, const int4* ri, const float4* rf,
       }
     } else if (t == XPBD_CONTACT) {
       int a = r.y, b = r.z;
-      float4 xa = x[a], xb = x[b];
+      const auto ea = pos(a);
+      const auto eb = pos(b);
+      float4 xa = ea.x, xb = eb.x;
       float wa = xa.w, wb = xb.w;
       float wsum = wa + wb;
       if (wsum != 0.0f) {
@@ -198,7 +274,7 @@ XD void row_jacobi(Pos x, const float4* xp, const int4* ri, const float4* rf,
             V3 cb = (-n_hat) * (wb * dlam);
             float mu = f.z;
             if (mu > 0.0f) {
-              V3 dp_rel = ((v3(xa) + ca) - v3(xp[a])) - ((v3(xb) + cb) - v3(xp[b]));
+              V3 dp_rel = ((v3(xa) + ca) - v3(ea.prev())) - ((v3(xb) + cb) - v3(eb.prev()));
               V3 fc = friction_delta(dp_rel, n_hat, -C, mu);
               ca = ca + fc * (wa / wsum);
               cb = cb - fc * (wb / wsum);
@@ -325,7 +401,7 @@ __global__ void k3_jacobi(Dev3 s, float h) {
   int m = *s.n_rows;
   AccGlobal acc{s.acc};
   for (int j = gtid(); j < m; j += gstride())
-    row_jacobi<FIRST>(PosPlain{s.x}, s.xp, s.ri, s.rf, s.ra, s.lam, j, h, acc);
+    row_jacobi<FIRST>(PosPlain{s.x, s.xp}, s.ri, s.rf, s.ra, s.lam, j, h, acc);
 }
 __global__ void k3_apply(Dev3 s, float relax) {
   for (int i = gtid(); i < s.n; i += gstride()) body_apply(s.x, s.acc, i, relax);
@@ -408,7 +484,91 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
       c_lam[k] = s.lam[j];
     }
   }
-  for (int f = 0; f < frames; ++f) {
+  // Folded substep boundaries (Jacobi, 2-4 iterations, latency-bound scenes):
+  // substep s's predicted state lives in buffer (s + 1) & 1 (0: x / x_prev; 1:
+  // the carry buffers behind the accumulators).  The first iteration of a
+  // substep reads the previous substep's state through PosCarry (the frame
+  // start through PosStart) while the owners of the particles store this
+  // substep's state; iteration k reads it with the corrections of iterations
+  // 0..k-1 (PosFolded).  The accumulators come in two sets (substep parity); a
+  // set is cleared in the second iteration of the next substep.  A substep
+  // has I barriers; the frame ends with one pass that applies, finalizes and
+  // stores the frame state.
+  const bool carry_path = !GS && !SMEM && p.fold && p.carry && m > 0;
+  auto rows_first = [&](const auto& pos, const AccGlobal& acc) {
+    if (cache_rows) {
+#pragma unroll
+      for (int k = 0; k < kCachedRows; ++k) {
+        const int j = tid0 + k * stride;
+        if (j < m) row_jacobi<true>(pos, &c_ri[k], &c_rf[k], s.ra + j, &c_lam[k], 0, p.h, acc);
+      }
+    } else {
+      for (int j = tid0; j < m; j += stride) row_jacobi<true>(pos, s.ri, s.rf, s.ra, s.lam, j, p.h, acc);
+    }
+  };
+  if (carry_path) {
+    const size_t st = (size_t)g.acc_stride;
+    const int I = p.iterations;
+    float4* const x1 = g.accs + (size_t)(2 * I) * st;
+    float4* const xp1 = g.accs + (size_t)(2 * I + 1) * st;
+    for (int f = 0; f < frames; ++f) {
+      for (int sub = 0; sub < p.substeps; ++sub) {
+        const int cur = (sub + 1) & 1, prv = sub & 1;
+        float4* const xc = cur ? x1 : s.x;    // this substep's state
+        float4* const xpc = cur ? xp1 : s.xp;
+        float4* const A = g.accs + (size_t)(prv * I) * st;    // this substep's set
+        float4* const Ap = g.accs + (size_t)(cur * I) * st;   // the previous substep's set
+        const PosStart start{s.x, s.v, p.h, gv};
+        const PosCarry carry{cur ? s.x : x1, cur ? s.xp : xp1, Ap, st, I, p.cap_on, p.relax, p.h, p.damping,
+                             p.max_speed, gv};
+        for (int it = 0; it < I; ++it) {
+          const AccGlobal acc_it{A + (size_t)it * st};
+          if (it == 0) {
+            for (int i = tid0; i < n; i += stride) {
+              const EndHeld e = sub == 0 ? start(i) : carry(i);
+              xc[i] = e.x;
+              xpc[i] = e.p;
+            }
+            if (sub == 0) rows_first(start, acc_it);
+            else rows_first(carry, acc_it);
+          } else {
+            if (it == 1 && sub > 0) {
+              for (int i = tid0; i < n; i += stride)
+                for (int k = 0; k < I; ++k) Ap[k * st + i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+            const PosFolded pos{xc, xpc, A, st, it, p.relax};
+            if (cache_rows) {
+#pragma unroll
+              for (int k = 0; k < kCachedRows; ++k) {
+                const int j = tid0 + k * stride;
+                if (j < m) row_jacobi<false>(pos, &c_ri[k], &c_rf[k], s.ra + j, &c_lam[k], 0, p.h, acc_it);
+              }
+            } else {
+              for (int j = tid0; j < m; j += stride) row_jacobi<false>(pos, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
+            }
+          }
+          sync();
+        }
+      }
+      // the last substep: every correction in order, finalize + clamp, frame state
+      const bool odd = p.substeps & 1;  // the last substep's state: buffer 1 when the count is odd
+      float4* const A = g.accs + (size_t)((odd ? 0 : 1) * I) * st;
+      for (int i = tid0; i < n; i += stride) {
+        float4 xi = (odd ? x1 : s.x)[i];
+        const float4 xpi = (odd ? xp1 : s.xp)[i];
+        float4 a[kMaxFoldIters];
+        load_accs(A, st, I, i, a);
+        xi = apply_accs(xi, a, I, p.relax);
+        for (int k = 0; k < I; ++k) A[k * st + i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const V3 vi = finalize_vel(xi, xpi, p.h, p.damping, p.cap_on, p.max_speed);
+        s.x[i] = xi;
+        s.xp[i] = xpi;
+        s.v[i] = f4(vi, 0.0f);
+      }
+      if (f + 1 < frames) sync();
+    }
+  }
+  for (int f = 0; f < (carry_path ? 0 : frames); ++f) {
     for (int i = tid0; i < n; i += stride) body_integrate(s.x, s.v, s.xp, i, p.h, gv);
     sync();
     for (int sub = 0; sub < p.substeps; ++sub) {
@@ -428,28 +588,28 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
           } else if (!SMEM && p.fold) {
             // folded Jacobi: read x plus the earlier iterations' averaged corrections,
             // accumulate into this iteration's own buffer; no apply phase
-            const PosFolded pos{s.x, g.accs, (size_t)g.acc_stride, it, p.relax};
+            const PosFolded pos{s.x, s.xp, g.accs, (size_t)g.acc_stride, it, p.relax};
             const AccGlobal acc_it{g.accs + (size_t)it * g.acc_stride};
             if (cache_rows) {
 #pragma unroll
               for (int k = 0; k < kCachedRows; ++k) {
                 const int j = tid0 + k * stride;
                 if (j < m) {
-                  if (it == 0) row_jacobi<true>(pos, s.xp, &c_ri[k], &c_rf[k], s.ra + j, &c_lam[k], 0, p.h, acc_it);
-                  else row_jacobi<false>(pos, s.xp, &c_ri[k], &c_rf[k], s.ra + j, &c_lam[k], 0, p.h, acc_it);
+                  if (it == 0) row_jacobi<true>(pos, &c_ri[k], &c_rf[k], s.ra + j, &c_lam[k], 0, p.h, acc_it);
+                  else row_jacobi<false>(pos, &c_ri[k], &c_rf[k], s.ra + j, &c_lam[k], 0, p.h, acc_it);
                 }
               }
             } else {
               for (int j = tid0; j < m; j += stride) {
-                if (it == 0) row_jacobi<true>(pos, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
-                else row_jacobi<false>(pos, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
+                if (it == 0) row_jacobi<true>(pos, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
+                else row_jacobi<false>(pos, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_it);
               }
             }
             sync();
           } else {
             for (int j = tid0; j < m; j += stride) {
-              if (it == 0) row_jacobi<true>(PosPlain{s.x}, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
-              else row_jacobi<false>(PosPlain{s.x}, s.xp, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
+              if (it == 0) row_jacobi<true>(PosPlain{s.x, s.xp}, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
+              else row_jacobi<false>(PosPlain{s.x, s.xp}, s.ri, s.rf, s.ra, s.lam, j, p.h, acc_fn);
             }
             sync();
             if (it + 1 < p.iterations) {
@@ -463,14 +623,12 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
       for (int i = tid0; i < n; i += stride) {
         if (!GS && !SMEM && p.fold && m > 0 && p.iterations > 0) {
           // every iteration's averaged correction in order, as apply_jacobi would
+          float4 a[kMaxFoldIters];
           float4 xi = s.x[i];
-          for (int it = 0; it < p.iterations; ++it) {
-            float4* ap = g.accs + (size_t)it * g.acc_stride + i;
-            float4 a = *ap;
-            *ap = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            int c = (int)a.w;
-            if (c > 0 && xi.w > 0.0f) xi = f4(v3(xi) + v3(a) * (p.relax / (float)c), xi.w);
-          }
+          load_accs(g.accs, (size_t)g.acc_stride, p.iterations, i, a);
+          xi = apply_accs(xi, a, p.iterations, p.relax);
+          for (int it = 0; it < p.iterations; ++it)
+            g.accs[(size_t)it * g.acc_stride + i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
           s.x[i] = xi;
         } else if (!GS && m > 0 && p.iterations > 0) {
           body_apply(s.x, s.acc, i, p.relax);
@@ -597,9 +755,27 @@ struct xpbd3_solver {
   int force_mode = -1, force_blocks = 0, force_threads = 0;
   float4* accs = nullptr;  // folded Jacobi accumulators (zero between launches)
   size_t accs_bytes = 0;
+  // attached contact rebuild (xpbd3_attach_contacts) and the captured frame
+  struct {
+    xpbd3_contacts* c;
+    const float *radius, *friction, *x_init;
+    const int* coll;
+    const int64_t* existing;
+    int n_coll, n_existing;
+    double margin, dt, rmax;
+    int* status;
+  } hook{};
+  bool hooked = false;
+  cudaGraphExec_t graph = nullptr;
 };
 
+static void free_graph3(xpbd3_solver* h) {
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+}
+
 static constexpr size_t kSmemMax = 227 * 1024;
+static constexpr long long kCarryMaxWork = 16LL * 1024 * 8;  // bodies or rows
 
 template <bool GS, bool SMEM>
 static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream) {
@@ -704,6 +880,7 @@ extern "C" int xpbd3_create(xpbd3_solver** out) {
 
 extern "C" int xpbd3_destroy(xpbd3_solver* h) {
   if (!h) return XPBD_OK;
+  free_graph3(h);
   if (h->bar) cudaFree(h->bar);
   if (h->accs) cudaFree(h->accs);
   delete h;
@@ -724,6 +901,8 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   if (!h || check_state(s) || !p) return XPBD_ERR_BAD_ARG;
   if (p->substeps < 0 || p->iterations < 0) return XPBD_ERR_BAD_ARG;
   if (p->gs && s->row_capacity > 0 && (!s->color_order || !s->color_starts)) return XPBD_ERR_BAD_ARG;
+  free_graph3(h);
+  h->hooked = false;
   h->st = *s;
   h->par = *p;
   h->dev = make_dev3(s);
@@ -758,11 +937,17 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   }
   // Jacobi on the cluster / grid drivers with 2-4 iterations: fold each apply
   // into the next iteration's reads (one barrier per iteration instead of two)
+  // Scenes small enough that the phases are latency-bound also fold the
+  // substep boundary into the first iteration's reads (I barriers per
+  // substep): two accumulator sets plus a second x / x_prev buffer.
   q.fold = 0;
+  q.carry = 0;
   h->dev.accs = nullptr;
   h->dev.acc_stride = 0;
-  if (!p->gs && mode != 1 && p->iterations >= 2 && p->iterations <= 4 && s->n_bodies > 0) {
-    size_t bytes = sizeof(float4) * (size_t)s->n_bodies * (size_t)p->iterations;
+  if (!p->gs && mode != 1 && p->iterations >= 2 && p->iterations <= kMaxFoldIters && s->n_bodies > 0) {
+    const int carry = work <= kCarryMaxWork ? 1 : 0;
+    const size_t bufs = carry ? 2 * (size_t)p->iterations + 2 : (size_t)p->iterations;
+    size_t bytes = sizeof(float4) * (size_t)s->n_bodies * bufs;
     if (bytes > h->accs_bytes) {
       if (h->accs) cudaFree(h->accs);
       h->accs = nullptr;
@@ -774,6 +959,7 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
     h->dev.accs = h->accs;
     h->dev.acc_stride = s->n_bodies;
     q.fold = 1;
+    q.carry = carry;
   }
   int rc;
   if (p->gs) rc = mode == 1 ? configure<true, true>(h) : configure<true, false>(h);
@@ -781,13 +967,62 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   return rc;
 }
 
+static int run_frames(xpbd3_solver* h, int frames, cudaStream_t st) {
+  const bool sm = h->mode == 1;
+  if (h->par.gs) return sm ? launch_frames<true, true>(h, frames, st) : launch_frames<true, false>(h, frames, st);
+  return sm ? launch_frames<false, true>(h, frames, st) : launch_frames<false, false>(h, frames, st);
+}
+
 extern "C" int xpbd3_step(xpbd3_solver* h, int frames, void* stream) {
   if (!h || frames < 0) return XPBD_ERR_BAD_ARG;
   if (frames == 0 || h->st.n_bodies == 0) return XPBD_OK;
   cudaStream_t st = as_stream(stream);
-  const bool sm = h->mode == 1;
-  if (h->par.gs) return sm ? launch_frames<true, true>(h, frames, st) : launch_frames<true, false>(h, frames, st);
-  return sm ? launch_frames<false, true>(h, frames, st) : launch_frames<false, false>(h, frames, st);
+  if (!h->hooked) return run_frames(h, frames, st);
+  // one frame = contact rebuild + frame kernel, captured once and replayed
+  if (!h->graph) {
+    const auto& k = h->hook;
+    cudaStream_t cap;
+    XPBD_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      cudaStreamDestroy(cap);
+      set_last_error("cudaStreamBeginCapture", e);
+      return XPBD_ERR_CUDA;
+    }
+    int rc = xpbd3_contacts_build(k.c, &h->st, k.radius, k.friction, k.coll, k.n_coll, k.existing, k.n_existing,
+                                  k.x_init, k.margin, k.dt, k.rmax, k.status, cap);
+    if (!rc) rc = run_frames(h, 1, cap);
+    e = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (rc) {
+      if (e == cudaSuccess) cudaGraphDestroy(g);
+      return rc;
+    }
+    XPBD_CUDA(e);
+    e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    XPBD_CUDA(e);
+  }
+  for (int f = 0; f < frames; ++f) XPBD_CUDA(cudaGraphLaunch(h->graph, st));
+  return XPBD_OK;
+}
+
+extern "C" int xpbd3_attach_contacts(xpbd3_solver* h, xpbd3_contacts* c, const float* radius,
+                                     const float* friction, const int* collide_idx, int n_collide,
+                                     const int64_t* existing, int n_existing, const float* x_init,
+                                     double contact_margin, double dt, double r_max, int* status_dev) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  free_graph3(h);
+  h->hooked = false;
+  if (!c) return XPBD_OK;
+  if (h->par.gs || !radius || !friction || !x_init || !status_dev || n_collide < 0 || n_existing < 0 ||
+      (n_collide > 0 && !collide_idx) || (n_existing > 0 && !existing))
+    return XPBD_ERR_BAD_ARG;
+  h->hook = {c, radius, friction, x_init, collide_idx, existing, n_collide, n_existing,
+             contact_margin, dt, r_max, status_dev};
+  h->hooked = true;
+  return XPBD_OK;
 }
 
 extern "C" int xpbd3_status(xpbd3_solver* h, int* out, void* stream) {

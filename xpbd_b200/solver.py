@@ -329,7 +329,8 @@ class Solver:
         return tune3(self, frames, candidates)
 
     def _bind(self) -> None:
-        self.binds = getattr(self, "binds", 0) + 1  # handle (re)binds: each one re-captures the frame graph
+        self.binds = getattr(self, "binds", 0) + 1  # handle (re)binds (a bind drops the captured frame)
+        self._hooked = False
         L = N.lib()
         if self._h is None:
             h = C.c_void_p()
@@ -348,8 +349,35 @@ class Solver:
         L = N.lib()
         stream = N.stream_of(self.device)
         if self._self_collision:
+            if not self.sync_contacts and self.solve_mode != "gs":
+                # contact rebuild + frame kernel as one captured CUDA graph per bind
+                if not self._hooked:
+                    self._attach_contacts(stream)
+                N.check(L.xpbd3_step(self._h, 1, stream), "xpbd3_step")
+                return
+            self._detach_contacts()
             self._build_contacts(stream)
         N.check(L.xpbd3_step(self._h, 1, stream), "xpbd3_step")
+
+    def _attach_contacts(self, stream) -> None:
+        """Hand the contact rebuild to the bound handle, so xpbd3_step runs it
+        before every frame inside one captured graph.  One plain rebuild first
+        (idempotent on the state) initialises the builder outside the capture."""
+        T = self._t
+        L = N.lib()
+        args = (N.ptr(T["radius"]), N.ptr(T["friction"]), N.ptr(T["collide_idx"]), int(T["collide_idx"].numel()),
+                N.ptr(T["existing"]), int(T["existing"].numel()), N.ptr(T["x_init"]),
+                C.c_double(self._contact_margin), C.c_double(self.dt), C.c_double(self._rmax), N.ptr(T["status"]))
+        N.check(L.xpbd3_contacts_build(self._contacts, C.byref(self._st), *args, stream), "xpbd3_contacts_build")
+        N.check(L.xpbd3_attach_contacts(self._h, self._contacts, *args), "xpbd3_attach_contacts")
+        self._hooked = True
+
+    def _detach_contacts(self) -> None:
+        """xpbd3_step runs the frame kernel alone again (contacts built by the caller)."""
+        if self._hooked:
+            N.check(N.lib().xpbd3_attach_contacts(self._h, None, None, None, None, 0, None, 0, None, 0.0, 0.0, 0.0,
+                                                  None), "xpbd3_attach_contacts")
+            self._hooked = False
 
     def step_frames(self, frames: int) -> None:
         """Advance `frames` frames in one launch (scenes without self collision)."""
