@@ -254,6 +254,7 @@ constexpr int kFusedMaxCollide = 4096;
 // the order a stable sort by cell id gives them (solver.py:514-562), without
 // the sort.
 constexpr uint64_t kEmptyCell = ~0ull;
+constexpr int kFusedPairCache = 4;  // pairs a thread keeps in registers between counting and writing
 
 struct FusedView {
   float4* pos;       // per collidable: sanitized position, radius
@@ -331,6 +332,9 @@ __global__ void __launch_bounds__(1024, 1) kc_fused(ContactArgs a) {
   __shared__ int s_warp[32];
   __shared__ int s_cta_total;
   __shared__ int s_scan[33];
+  // a frame kernel launched as this grid's programmatic dependent may start
+  // its launch now; it waits for this grid's completion before reading
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const unsigned rank = cluster_rank(), csize = cluster_size();
   const int m = a.m;
@@ -390,6 +394,9 @@ __global__ void __launch_bounds__(1024, 1) kc_fused(ContactArgs a) {
     if (!finite3(p)) p = a.x_init[g];
     f.pos[k] = make_float4(p.x, p.y, p.z, a.radius[g]);
     int c[3] = {(int)floorf(p.x / cell), (int)floorf(p.y / cell), (int)floorf(p.z / cell)};
+    cslot[k] = c[0];  // the cell coordinates, until the table takes these arrays over
+    ticket[k] = c[1];
+    f.member[k] = c[2];
     for (int d = 0; d < 3; ++d) {
       lmin[d] = min(lmin[d], c[d]);
       lmax[d] = max(lmax[d], c[d]);
@@ -416,15 +423,13 @@ __global__ void __launch_bounds__(1024, 1) kc_fused(ContactArgs a) {
     red.cmax[d] = s_max[d];
   }
   const int64_t S = grid_S(&red);
-  auto cid_of = [&](int k) {
-    float4 p = f.pos[k];
-    int64_t cx = (int64_t)(int)floorf(p.x / cell) - red.cmin[0], cy = (int64_t)(int)floorf(p.y / cell) - red.cmin[1],
-            cz = (int64_t)(int)floorf(p.z / cell) - red.cmin[2];
-    return (cx * S + cy) * S + cz;
-  };
+  // a collidable's cell id: its slot's key once the table is built
+  auto cid_of = [&](int k) { return (int64_t)f.key[cslot[k]]; };
   // 3. cell table: insert every collidable's cell, count its members
   for (int k = tid; k < m; k += 1024) {
-    const uint64_t cid = (uint64_t)cid_of(k);
+    const int64_t cx = (int64_t)cslot[k] - red.cmin[0], cy = (int64_t)ticket[k] - red.cmin[1],
+                  cz = (int64_t)f.member[k] - red.cmin[2];
+    const uint64_t cid = (uint64_t)((cx * S + cy) * S + cz);
     const unsigned mask = (unsigned)H - 1u;
     unsigned h = cell_hash(cid, f.hbits);
     for (unsigned p = 0; p <= mask; ++p) {
@@ -474,10 +479,19 @@ __global__ void __launch_bounds__(1024, 1) kc_fused(ContactArgs a) {
   const int c0 = min((int)rank * per_cta, slots), c1 = min(c0 + per_cta, slots);
   const int per = (c1 - c0 + 1023) / 1024;
   const int t0 = min(c0 + tid * per, c1), t1 = min(t0 + per, c1);
+  // the thread's first kFusedPairCache pairs stay in registers for step 6
   int mine = 0;
+  int2 pc[kFusedPairCache];
+#pragma unroll
+  for (int q = 0; q < kFusedPairCache; ++q) pc[q] = make_int2(0, 0);
   for (int t = t0; t < t1; ++t) {
     const int o = t / m, k = t - o * m;
-    int c = visit_slot_fused(a, f, o, k, cid_of(k), marg, S, [](int, int, int) {});
+    const int before = mine;
+    int c = visit_slot_fused(a, f, o, k, cid_of(k), marg, S, [&](int r, int ga, int gb) {
+#pragma unroll
+      for (int q = 0; q < kFusedPairCache; ++q)
+        if (q == before + r) pc[q] = make_int2(ga, gb);
+    });
     if (c) atomicOr(&nonempty[t >> 5], 1u << (t & 31));
     mine += c;
   }
@@ -499,43 +513,52 @@ __global__ void __launch_bounds__(1024, 1) kc_fused(ContactArgs a) {
     if (lane == 31) s_cta_total = wi;
   }
   cluster_sync_all();  // every CTA's total is visible, and no CTA reads x or v any more
-  if (rank == 0) {
-    for (int i = tid; i < a.n; i += 1024) {
-      float4 xi = a.x[i];
-      if (!finite3(xi)) {
-        float4 x0 = a.x_init[i];
-        a.x[i] = make_float4(x0.x, x0.y, x0.z, xi.w);
-        a.v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        raise_status(a.status, XPBD_ERR_NAN);
-      }
-    }
+  // every CTA's total at once (lane q reads CTA q), then the sums over the warp
+  int tq = lane < (int)csize ? ld_cluster_int(&s_cta_total, (unsigned)lane) : 0;
+  int cta_base = lane < (int)rank ? tq : 0, total = tq;
+  for (int o = 16; o; o >>= 1) {
+    cta_base += __shfl_xor_sync(0xffffffffu, cta_base, o);
+    total += __shfl_xor_sync(0xffffffffu, total, o);
   }
-  int cta_base = 0, total = 0;
-  for (unsigned q = 0; q < csize; ++q) {
-    int tq = ld_cluster_int(&s_cta_total, q);
-    if (q < rank) cta_base += tq;
-    total += tq;
-  }
-  cluster_sync_all();  // no CTA leaves while another may still read its total
+  cluster_arrive();  // no CTA leaves (cluster_wait at the end) while another may still read its total
   int base = cta_base + s_warp[warp] + inc - mine;
   if (rank == 0 && tid == 0) {
     *a.n_rows = a.n_static + min(total, a.cap_contacts);
     if (total > a.cap_contacts) raise_status(a.status, XPBD_ERR_OVERFLOW);
   }
-  // 6. write the rows of this thread's slots at their offsets
-  for (int t = t0; t < t1; ++t) {
-    if (!(nonempty[t >> 5] & (1u << (t & 31)))) continue;
-    const int o = t / m, k = t - o * m;
-    const int b0 = base;
-    base += visit_slot_fused(a, f, o, k, cid_of(k), marg, S, [&](int r, int ga, int gb) {
-      int slot = b0 + r;
-      if (slot >= a.cap_contacts) return;
-      int row = a.n_static + slot;
-      a.ri[row] = make_int4(XPBD_CONTACT, ga, gb, 1);
-      a.rf[row] = make_float4(a.radius[ga] + a.radius[gb], 0.0f, sqrtf(a.friction[ga] * a.friction[gb]), 0.0f);
-      a.ra[row] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    });
+  // 6. write the rows of this thread's slots at their offsets (from the
+  // registers, or a second visit when the thread found more pairs)
+  auto put = [&](int slot, int ga, int gb) {
+    if (slot >= a.cap_contacts) return;
+    int row = a.n_static + slot;
+    a.ri[row] = make_int4(XPBD_CONTACT, ga, gb, 1);
+    a.rf[row] = make_float4(a.radius[ga] + a.radius[gb], 0.0f, sqrtf(a.friction[ga] * a.friction[gb]), 0.0f);
+    a.ra[row] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  };
+  if (mine <= kFusedPairCache) {
+#pragma unroll
+    for (int q = 0; q < kFusedPairCache; ++q)
+      if (q < mine) put(base + q, pc[q].x, pc[q].y);
+  } else {
+    for (int t = t0; t < t1; ++t) {
+      if (!(nonempty[t >> 5] & (1u << (t & 31)))) continue;
+      const int o = t / m, k = t - o * m;
+      const int b0 = base;
+      base += visit_slot_fused(a, f, o, k, cid_of(k), marg, S, [&](int r, int ga, int gb) { put(b0 + r, ga, gb); });
+    }
   }
+  // the sanitized positions, written back by all CTAs (each index once; no
+  // CTA reads x or v after the first cluster barrier)
+  for (int i = (int)rank * 1024 + tid; i < a.n; i += (int)csize * 1024) {
+    float4 xi = a.x[i];
+    if (!finite3(xi)) {
+      float4 x0 = a.x_init[i];
+      a.x[i] = make_float4(x0.x, x0.y, x0.z, xi.w);
+      a.v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      raise_status(a.status, XPBD_ERR_NAN);
+    }
+  }
+  cluster_wait();
 }
 
 __global__ void kc_no_contacts(ContactArgs a) {

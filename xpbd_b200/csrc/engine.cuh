@@ -125,6 +125,10 @@ XD void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
+// The two halves of cluster_sync_all, for work between the arrival and the
+// wait (every thread of the cluster calls each once, in this order).
+XD void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+XD void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
 // Loads an int from the shared memory of CTA `rank` of this cluster.
 XD int ld_cluster_int(const int* local, unsigned rank) {
   unsigned addr = (unsigned)__cvta_generic_to_shared(local), remote;

@@ -436,6 +436,10 @@ template <bool GS, bool SMEM>
 __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p, int frames, GridBarrier bar) {
   extern __shared__ float4 smem[];
   const int n = g.n;
+  // launched as a programmatic dependent of the contact builder (captured
+  // frame): wait here until the builder's rows and positions are complete and
+  // visible (a no-op for an ordinary launch)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const int m = *g.n_rows;
   Dev3 s = g;
   if (SMEM) {
@@ -778,7 +782,7 @@ static constexpr size_t kSmemMax = 227 * 1024;
 static constexpr long long kCarryMaxWork = 16LL * 1024 * 8;  // bodies or rows
 
 template <bool GS, bool SMEM>
-static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream) {
+static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream, bool after_builder) {
   GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2), h->mode == 2 ? 1 : 0};
   auto kern = k3_frames<GS, SMEM>;
   cudaLaunchConfig_t cfg = {};
@@ -786,7 +790,7 @@ static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream) {
   cfg.blockDim = dim3(h->threads);
   cfg.dynamicSmemBytes = h->smem;
   cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   if (h->mode == 2) {
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = h->blocks;
@@ -798,6 +802,14 @@ static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream) {
   }
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  // Right after the contact builder (cluster and single-CTA drivers): the
+  // launch overlaps the builder's tail; the kernel's griddepcontrol.wait holds
+  // it until the builder has finished.
+  if (after_builder && h->mode != 0) {
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.numAttrs = 2;
+  }
   cudaError_t e = cudaLaunchKernelEx(&cfg, kern, h->dev, h->p3, frames, gb);
   if (e != cudaSuccess) {
     char what[160];
@@ -967,10 +979,13 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   return rc;
 }
 
-static int run_frames(xpbd3_solver* h, int frames, cudaStream_t st) {
+static int run_frames(xpbd3_solver* h, int frames, cudaStream_t st, bool after_builder = false) {
   const bool sm = h->mode == 1;
-  if (h->par.gs) return sm ? launch_frames<true, true>(h, frames, st) : launch_frames<true, false>(h, frames, st);
-  return sm ? launch_frames<false, true>(h, frames, st) : launch_frames<false, false>(h, frames, st);
+  if (h->par.gs)
+    return sm ? launch_frames<true, true>(h, frames, st, after_builder)
+              : launch_frames<true, false>(h, frames, st, after_builder);
+  return sm ? launch_frames<false, true>(h, frames, st, after_builder)
+            : launch_frames<false, false>(h, frames, st, after_builder);
 }
 
 extern "C" int xpbd3_step(xpbd3_solver* h, int frames, void* stream) {
@@ -992,7 +1007,7 @@ extern "C" int xpbd3_step(xpbd3_solver* h, int frames, void* stream) {
     }
     int rc = xpbd3_contacts_build(k.c, &h->st, k.radius, k.friction, k.coll, k.n_coll, k.existing, k.n_existing,
                                   k.x_init, k.margin, k.dt, k.rmax, k.status, cap);
-    if (!rc) rc = run_frames(h, 1, cap);
+    if (!rc) rc = run_frames(h, 1, cap, true);
     e = cudaStreamEndCapture(cap, &g);
     cudaStreamDestroy(cap);
     if (rc) {
