@@ -58,14 +58,38 @@ XD uint64_t global_ns() {
 // Every wait gives up after ~2 s of wall time, sets XPBD_ERR_BARRIER_TIMEOUT in
 // the status word and returns; once the bit is set no barrier waits again, so a
 // kernel can never hang on it.  With one block it is a plain __syncthreads().
+// Grid-wide barrier of a cooperative launch (or the hardware barrier when the
+// grid is one thread-block cluster).  The software form is a ticket barrier:
+// the arrival count (64 bits) only grows, every CTA arrives once at every
+// barrier, so a barrier completes when the count reaches the next multiple of
+// the grid size -- one release atomic per CTA and acquire polls, no reset on
+// the critical path.  Every CTA calls grid_exit at the end of the kernel; the
+// last one resets the count, so each launch starts from zero whatever grid
+// size it has.  Words: [0..1] count, [2] status, [3] exits.
 struct GridBarrier {
-  unsigned* count;  // arrivals at the current barrier
-  unsigned* gen;    // generation number
+  unsigned long long* count;
   int* status;
-  int cluster;      // 1: the grid is one thread-block cluster -> hardware cluster barrier
+  unsigned* exits;
+  int cluster;  // 1: the grid is one thread-block cluster -> hardware cluster barrier
 };
 
+inline GridBarrier make_grid_barrier(unsigned* words, int cluster) {
+  return GridBarrier{reinterpret_cast<unsigned long long*>(words), reinterpret_cast<int*>(words + 2), words + 3,
+                     cluster};
+}
+
 constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;
+
+XD unsigned long long atom_add_release_gpu(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+XD unsigned long long ld_acquire_gpu(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
 
 XD void grid_sync(const GridBarrier& b) {
   if (gridDim.x == 1) {
@@ -79,31 +103,47 @@ XD void grid_sync(const GridBarrier& b) {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
     return;
   }
+  // Ordering without fences: the CTA's writes precede thread 0's arrival
+  // through __syncthreads, the arrival is a gpu-scope release, the polls are
+  // gpu-scope acquires, and the closing __syncthreads passes the acquire on to
+  // the CTA (a base-causality chain of the PTX memory model).
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* vgen = b.gen;
+    const unsigned long long N = gridDim.x;
+    const unsigned long long prev = atom_add_release_gpu(b.count, 1ull);
+    const unsigned long long target = prev - prev % N + N;
     volatile int* vstat = b.status;
-    unsigned g = *vgen;
-    __threadfence();
-    unsigned prev = atomicAdd(b.count, 1u);
-    if (prev == gridDim.x - 1) {
-      atomicExch(b.count, 0u);
-      __threadfence();
-      atomicAdd(b.gen, 1u);
-    } else if ((*vstat & XPBD_ERR_BARRIER_TIMEOUT) == 0) {
-      uint64_t t0 = global_ns();
-      while (*vgen == g) {
+    uint64_t t0 = 0;
+    unsigned spins = 0;
+    while (ld_acquire_gpu(b.count) < target) {
+      if ((++spins & 255u) == 0u) {  // now and then: a barrier that already gave up, or the time limit
         if (*vstat & XPBD_ERR_BARRIER_TIMEOUT) break;
-        if (global_ns() - t0 > kBarrierTimeoutNs) {
+        const uint64_t t = global_ns();
+        if (t0 == 0) {
+          t0 = t;
+        } else if (t - t0 > kBarrierTimeoutNs) {
           atomicOr(b.status, XPBD_ERR_BARRIER_TIMEOUT);
           break;
         }
-        __nanosleep(32);
       }
+      __nanosleep(32);
     }
-    __threadfence();
   }
   __syncthreads();
+}
+
+// End of a kernel that used grid_sync: the last CTA out resets the count (no
+// CTA polls it any more once every CTA has arrived here).
+XD void grid_exit(const GridBarrier& b) {
+  if (gridDim.x == 1 || b.cluster) return;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(b.exits, 1u) == gridDim.x - 1) {
+      *b.count = 0ull;
+      *b.exits = 0u;
+      __threadfence();
+    }
+  }
 }
 
 // grid-stride helpers

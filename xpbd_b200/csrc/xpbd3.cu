@@ -658,6 +658,7 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
       if (j < m) g.lam[j] = c_lam[k];
     }
   }
+  if (!SMEM) grid_exit(bar);
 }
 
 }  // namespace xpbd
@@ -783,7 +784,7 @@ static constexpr long long kCarryMaxWork = 16LL * 1024 * 8;  // bodies or rows
 
 template <bool GS, bool SMEM>
 static int launch_frames(xpbd3_solver* h, int frames, cudaStream_t stream, bool after_builder) {
-  GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2), h->mode == 2 ? 1 : 0};
+  const GridBarrier gb = make_grid_barrier(h->bar, h->mode == 2 ? 1 : 0);
   auto kern = k3_frames<GS, SMEM>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(h->blocks);

@@ -1001,6 +1001,7 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
     }
     grid_sync(bar);
   }
+  grid_exit(bar);
 }
 
 // Persistent substep kernel, quarter-warp phases (manifold, floor, box,
@@ -1055,6 +1056,7 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
     }
     grid_sync(bar);
   }
+  grid_exit(bar);
 }
 
 __global__ void k6_manifold8(Dev6 s, float margin) {
@@ -2498,7 +2500,7 @@ static int run_broadphase(xpbd6_solver* h, cudaStream_t st) {
 
 static int run_substeps(xpbd6_solver* h, cudaStream_t st) {
   if (h->dev.n == 0) return XPBD_OK;
-  GridBarrier gb{h->bar, h->bar + 1, reinterpret_cast<int*>(h->bar + 2), h->mode == 2 ? 1 : 0};
+  const GridBarrier gb = make_grid_barrier(h->bar, h->mode == 2 ? 1 : 0);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(h->blocks);
   cfg.blockDim = dim3(h->threads);
