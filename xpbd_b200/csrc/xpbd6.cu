@@ -394,20 +394,68 @@ XD void joint_row(const Dev6& s, int k, float h) {
 }
 
 // ---- kernels_6dof.py:487-535 apply_jacobi_6dof + finalize_velocity_6dof --------------
-XD void body_apply6(const Dev6& s, int i, float relax) {
-  float4 a = s.ax[i];
+// on values: translation and rotation averaged over the count, the orientation
+// renormalized
+XD void apply6(float4& x4, Q4& qi, float4 a, float4 r, float relax) {
   int n = (int)a.w;
-  float4 x4 = s.x[i];
   if (n > 0 && x4.w > 0.0f) {
     float inv_n = relax / (float)n;
-    s.x[i] = f4(v3(x4) + v3(a) * inv_n, x4.w);
-    V3 dw = v3(s.ar[i]) * inv_n;
-    Q4 qi = q4(s.q[i]);
+    x4 = f4(v3(x4) + v3(a) * inv_n, x4.w);
+    V3 dw = v3(r) * inv_n;
     Q4 pq = qmul(Q4{dw.x, dw.y, dw.z, 0.0f}, qi);
-    s.q[i] = f4(qnormalize(Q4{qi.x + 0.5f * pq.x, qi.y + 0.5f * pq.y, qi.z + 0.5f * pq.z, qi.w + 0.5f * pq.w}));
+    qi = qnormalize(Q4{qi.x + 0.5f * pq.x, qi.y + 0.5f * pq.y, qi.z + 0.5f * pq.z, qi.w + 0.5f * pq.w});
+  }
+}
+
+XD void body_apply6(const Dev6& s, int i, float relax) {
+  const float4 a = s.ax[i], r = s.ar[i], qv = s.q[i];
+  float4 x4 = s.x[i];
+  if ((int)a.w > 0 && x4.w > 0.0f) {
+    Q4 qi = q4(qv);
+    apply6(x4, qi, a, r, relax);
+    s.x[i] = x4;
+    s.q[i] = f4(qi);
   }
   s.ax[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   s.ar[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// finalize_velocity_6dof on values (x, q after the last apply; xp, qp the
+// substep start)
+XD void finalize6(const Dev6& s, int i, const Par6& p, float4 x4, Q4 qi, float4 xp4, float4 qp4) {
+  if (x4.w == 0.0f) {
+    s.v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    s.w[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    return;
+  }
+  s.v[i] = f4(((v3(x4) - v3(xp4)) / p.h) * (1.0f - p.lin_damp), 0.0f);
+  Q4 dq = qmul(qi, qconj(q4(qp4)));
+  V3 w = V3{dq.x, dq.y, dq.z} * (2.0f / p.h);
+  if (dq.w < 0.0f) w = -w;
+  s.w[i] = f4(w * (1.0f - p.ang_damp), 0.0f);
+}
+
+// The persistent kernels' per-body pass after an iteration: apply (and, after
+// the last iteration, finalize) with every load issued first and the stored
+// values carried on in registers -- the same expressions as body_apply6 then
+// body_finalize6.
+XD void body_apply_finalize6(const Dev6& s, int i, const Par6& p, bool fin) {
+  const float4 a = s.ax[i], r = s.ar[i], qv = s.q[i];
+  float4 x4 = s.x[i];
+  float4 xp4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), qp4 = xp4;
+  if (fin) {
+    xp4 = s.xp[i];
+    qp4 = s.qp[i];
+  }
+  Q4 qi = q4(qv);
+  if ((int)a.w > 0 && x4.w > 0.0f) {
+    apply6(x4, qi, a, r, p.relax);
+    s.x[i] = x4;
+    s.q[i] = f4(qi);
+  }
+  s.ax[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  s.ar[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (fin) finalize6(s, i, p, x4, qi, xp4, qp4);
 }
 
 XD void body_finalize6(const Dev6& s, int i, const Par6& p) {
@@ -546,6 +594,62 @@ XD void body_apply_velocity6(const Dev6& s, int i, const Par6& p) {
   s.w[i] = f4(wi, 0.0f);
 }
 
+// The persistent kernels' per-body pass after the velocity solve: apply the
+// averaged velocity corrections and clamp, then (when another substep follows)
+// integrate it, with every load issued first -- the same expressions as
+// body_apply_velocity6 then body_integrate6.
+XD void body_velocity_integrate6(const Dev6& s, int i, const Par6& p, bool more) {
+  const float4 a = s.av[i], aw4 = s.aw[i], v4 = s.v[i], w4 = s.w[i], x4 = s.x[i], qv = s.q[i];
+  const float4 I4 = p.gyro ? s.inv_I[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  int n = (int)a.w;
+  V3 vi = v3(v4), wi = v3(w4);
+  if (n > 0 && x4.w > 0.0f) {
+    float inv_n = 1.0f / (float)n;
+    vi = vi + v3(a) * inv_n;
+    wi = wi + v3(aw4) * inv_n;
+  }
+  s.av[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  s.aw[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (p.max_speed > 0.0f) {
+    float sp = length(vi);
+    if (sp > p.max_speed) vi = vi * (p.max_speed / sp);
+    float sa = length(wi);
+    if (p.max_omega > 0.0f && sa > p.max_omega) wi = wi * (p.max_omega / sa);
+  }
+  if (!more || x4.w == 0.0f) {
+    s.v[i] = f4(vi, 0.0f);
+    s.w[i] = f4(wi, 0.0f);
+    if (more) {  // a static body: integrate only records the substep start
+      s.xp[i] = x4;
+      s.qp[i] = qv;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) s.lam_floor[8 * i + c] = 0.0f;
+    }
+    return;
+  }
+  s.xp[i] = x4;
+  s.qp[i] = qv;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) s.lam_floor[8 * i + c] = 0.0f;
+  vi = vi + V3{p.gx, p.gy, p.gz} * p.h;
+  s.v[i] = f4(vi, 0.0f);
+  s.x[i] = f4(v3(x4) + vi * p.h, x4.w);
+  Q4 q = q4(qv);
+  if (p.gyro) {
+    V3 wb = qrot_inv(q, wi);
+    V3 ii = v3(I4);
+    float ix = ii.x > 0.0f ? 1.0f / ii.x : 0.0f;
+    float iy = ii.y > 0.0f ? 1.0f / ii.y : 0.0f;
+    float iz = ii.z > 0.0f ? 1.0f / ii.z : 0.0f;
+    V3 Iw = V3{ix * wb.x, iy * wb.y, iz * wb.z};
+    V3 tau = -cross(wb, Iw);
+    V3 dwb = V3{ii.x * tau.x, ii.y * tau.y, ii.z * tau.z} * p.h;
+    wi = wi + qrot(q, dwb);
+  }
+  s.w[i] = f4(wi, 0.0f);
+  s.q[i] = f4(quat_integrate(q, wi, p.h));
+}
+
 // =================================================================================
 // Quarter-warp variants: 8 lanes cooperate on one floor body (one lane per box
 // corner), one contact pair (one lane per manifold point) or one manifold
@@ -607,11 +711,12 @@ XD int gscan_ex(const Grp& G, int v, int* total) {  // exclusive prefix within t
 }
 
 XD void floor_body8(const Dev6& s, int i, const Par6& p, const Grp& G) {
-  float4 x4 = s.x[i];
+  // every load first (one round trip), then the arithmetic
+  const float4 x4 = s.x[i], q4i = s.q[i], he4 = s.he[i], I4 = s.inv_I[i], xp4 = s.xp[i], qp4 = s.qp[i];
   float im = x4.w;
   if (im == 0.0f) return;
-  V3 xi = v3(x4), he = v3(s.he[i]), Ii = v3(s.inv_I[i]);
-  Q4 qi = q4(s.q[i]);
+  V3 xi = v3(x4), he = v3(he4), Ii = v3(I4);
+  Q4 qi = q4(q4i);
   const V3 S = V3{0.0f, 1.0f, 0.0f};
   // normal (dx, dr) and friction (fx, fr) terms of this lane's corner
   V3 dx = V3{0.0f, 0.0f, 0.0f}, dr = V3{0.0f, 0.0f, 0.0f};
@@ -635,7 +740,7 @@ XD void floor_body8(const Dev6& s, int i, const Par6& p, const Grp& G) {
       dr = world_invI_mul(qi, Ii, cross(r, P));
       cnt = 1.0f;
       if (p.mu > 0.0f) {
-        V3 p1b = v3(s.xp[i]) + qrot(q4(s.qp[i]), corner);
+        V3 p1b = v3(xp4) + qrot(q4(qp4), corner);
         V3 dp = p1 - p1b;
         V3 dpt = dp - S * dot(dp, S);
         float lt = length(dpt);
@@ -660,11 +765,16 @@ XD void floor_body8(const Dev6& s, int i, const Par6& p, const Grp& G) {
 }
 
 XD void box_pair8(const Dev6& s, int pid, const Grp& G) {
+  // the pair's own records with the header (one round trip), the bodies next
+  const int c = G.l;
+  const int slot = 8 * pid + c;
   int4 hdr = s.m_hdr[pid];
+  const float4 nrm = s.m_normal[pid], off_inc = s.m_off_inc[slot], off_ref = s.m_off_ref[slot];
+  const float lam_slot = s.lam_pair[slot];
   const int nc = hdr.x;
   if (nc == 0) return;
   const int inc = hdr.y, ref = hdr.z;
-  V3 S = v3(s.m_normal[pid]);
+  V3 S = v3(nrm);
   float4 xi4 = s.x[inc], xr4 = s.x[ref];
   V3 xi = v3(xi4), xr = v3(xr4);
   Q4 qi = q4(s.q[inc]), qr = q4(s.q[ref]);
@@ -672,11 +782,9 @@ XD void box_pair8(const Dev6& s, int pid, const Grp& G) {
   const float imi = xi4.w, imr = xr4.w;
   V3 dxi = V3{0, 0, 0}, dri = V3{0, 0, 0}, dxr = V3{0, 0, 0}, drr = V3{0, 0, 0};
   float ci = 0.0f, cr = 0.0f;
-  const int c = G.l;
   if (c < nc) {
-    int slot = 8 * pid + c;
-    V3 p_inc = xi + qrot(qi, v3(s.m_off_inc[slot]));
-    V3 p_ref = xr + qrot(qr, v3(s.m_off_ref[slot]));
+    V3 p_inc = xi + qrot(qi, v3(off_inc));
+    V3 p_ref = xr + qrot(qr, v3(off_ref));
     float C = dot(p_inc - p_ref, S);
     if (C >= 0.0f) {
       s.lam_pair[slot] = 0.0f;
@@ -688,7 +796,7 @@ XD void box_pair8(const Dev6& s, int pid, const Grp& G) {
       float wsum = w_inc + w_ref;
       if (wsum > 0.0f) {
         float dlam = d / wsum;
-        s.lam_pair[slot] = s.lam_pair[slot] + dlam;
+        s.lam_pair[slot] = lam_slot + dlam;
         V3 P = S * dlam;
         if (imi > 0.0f) {
           dxi = P * imi;
@@ -722,16 +830,17 @@ XD void box_pair8(const Dev6& s, int pid, const Grp& G) {
 }
 
 XD void velocity_floor8(const Dev6& s, int i, const Par6& p, const Grp& G) {
-  float4 x4 = s.x[i];
+  // every load first (one round trip), then the arithmetic
+  const float4 x4 = s.x[i], q4i = s.q[i], I4 = s.inv_I[i], he4 = s.he[i], v4 = s.v[i], w4 = s.w[i];
+  const int c = G.l;
+  const float lam_n = s.lam_floor[8 * i + c];
   float im = x4.w;
   if (im == 0.0f) return;
   const V3 S = V3{0.0f, 1.0f, 0.0f};
-  Q4 qi = q4(s.q[i]);
-  V3 Ii = v3(s.inv_I[i]), he = v3(s.he[i]), vi = v3(s.v[i]), wi = v3(s.w[i]);
+  Q4 qi = q4(q4i);
+  V3 Ii = v3(I4), he = v3(he4), vi = v3(v4), wi = v3(w4);
   V3 dv = V3{0, 0, 0}, dw = V3{0, 0, 0};
   float cnt = 0.0f;
-  const int c = G.l;
-  float lam_n = s.lam_floor[8 * i + c];
   if (lam_n != 0.0f) {
     V3 r = qrot(qi, box_corner(he, c));
     V3 vc = vi + cross(wi, r);
@@ -756,11 +865,16 @@ XD void velocity_floor8(const Dev6& s, int i, const Par6& p, const Grp& G) {
 }
 
 XD void velocity_box8(const Dev6& s, int pid, const Par6& p, const Grp& G) {
+  // the pair's own records with the header (one round trip), the bodies next
+  const int c = G.l;
+  const int slot = 8 * pid + c;
   int4 hdr = s.m_hdr[pid];
+  const float4 nrm = s.m_normal[pid], off_i = s.m_off_inc[slot], off_j = s.m_off_ref[slot];
+  const float lam_slot = s.lam_pair[slot];
   const int nc = hdr.x;
   if (nc == 0) return;
   const int ci = hdr.y, cj = hdr.z;
-  V3 S = v3(s.m_normal[pid]);
+  V3 S = v3(nrm);
   float4 xi4 = s.x[ci], xj4 = s.x[cj];
   V3 xi = v3(xi4), xj = v3(xj4);
   Q4 qi = q4(s.q[ci]), qj = q4(s.q[cj]);
@@ -769,13 +883,11 @@ XD void velocity_box8(const Dev6& s, int pid, const Par6& p, const Grp& G) {
   const float imi = xi4.w, imj = xj4.w;
   V3 dvi = V3{0, 0, 0}, dwi = V3{0, 0, 0}, dvj = V3{0, 0, 0}, dwj = V3{0, 0, 0};
   float ni = 0.0f, nj = 0.0f;
-  const int c = G.l;
   if (c < nc) {
-    int slot = 8 * pid + c;
-    float lam_n = s.lam_pair[slot];
+    float lam_n = lam_slot;
     if (lam_n != 0.0f) {
-      V3 p_inc = xi + qrot(qi, v3(s.m_off_inc[slot]));
-      V3 p_ref = xj + qrot(qj, v3(s.m_off_ref[slot]));
+      V3 p_inc = xi + qrot(qi, v3(off_i));
+      V3 p_ref = xj + qrot(qj, v3(off_j));
       V3 ri = p_inc - xi, rj = p_ref - xj;
       V3 vrel = (vi + cross(wi, ri)) - (vj + cross(wj, rj));
       V3 impulse = velocity_impulse(vrel, S, lam_n, p);
@@ -977,10 +1089,7 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
       }
       grid_sync(bar);
       const bool last = it + 1 == p.iterations;
-      for (int i = t0; i < n; i += st) {
-        body_apply6(s, i, p.relax);
-        if (last) body_finalize6(s, i, p);
-      }
+      for (int i = t0; i < n; i += st) body_apply_finalize6(s, i, p, last);
       grid_sync(bar);
     }
     if (p.iterations == 0) {
@@ -993,10 +1102,7 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
     }
     grid_sync(bar);
     for (int i = t0; i < nb; i += st) {
-      if (i < n) {
-        body_apply_velocity6(s, i, p);
-        if (more) body_integrate6(s, i, p);
-      }
+      if (i < n) body_velocity_integrate6(s, i, p, more);
       if (more && i < nj) s.lam_joint[i] = 0.0f;
     }
     grid_sync(bar);
@@ -1032,10 +1138,7 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
       }
       grid_sync(bar);
       const bool last = it + 1 == p.iterations;
-      for (int i = t0; i < n; i += st) {
-        body_apply6(s, i, p.relax);
-        if (last) body_finalize6(s, i, p);
-      }
+      for (int i = t0; i < n; i += st) body_apply_finalize6(s, i, p, last);
       grid_sync(bar);
     }
     if (p.iterations == 0) {
@@ -1048,10 +1151,7 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
     }
     grid_sync(bar);
     for (int i = t0; i < nb; i += st) {
-      if (i < n) {
-        body_apply_velocity6(s, i, p);
-        if (more) body_integrate6(s, i, p);
-      }
+      if (i < n) body_velocity_integrate6(s, i, p, more);
       if (more && i < nj) s.lam_joint[i] = 0.0f;
     }
     grid_sync(bar);
