@@ -158,6 +158,22 @@ struct PosFolded {
     return EndLazy{apply_accs(xi, a, n_prev, relax), xp + i};
   }
 };
+// The same with the substep-start position loaded alongside (the latency-bound
+// scenes of the carry path: friction rows then wait on one round trip, not two).
+struct PosFoldedHeld {
+  const float4* x;
+  const float4* xp;
+  const float4* acc;
+  size_t stride;
+  int n_prev;
+  float relax;
+  XD EndHeld operator()(int i) const {
+    float4 a[kMaxFoldIters];
+    const float4 xi = x[i], xpi = xp[i];
+    load_accs(acc, stride, n_prev, i, a);
+    return EndHeld{apply_accs(xi, a, n_prev, relax), xpi};
+  }
+};
 // The substep boundary on the fly: the previous substep's predicted position x
 // and start position xp with every iteration's averaged correction applied in
 // order, the velocity finalized and clamped, then integrated into this substep
@@ -540,7 +556,7 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
               for (int i = tid0; i < n; i += stride)
                 for (int k = 0; k < I; ++k) Ap[k * st + i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             }
-            const PosFolded pos{xc, xpc, A, st, it, p.relax};
+            const PosFoldedHeld pos{xc, xpc, A, st, it, p.relax};
             if (cache_rows) {
 #pragma unroll
               for (int k = 0; k < kCachedRows; ++k) {
