@@ -45,6 +45,7 @@ struct Par3 {
   int cap_on, substeps, iterations, gs;
   int fold = 0;   // 1: Jacobi with the apply folded into the next iteration's reads
   int carry = 0;  // 1 (with fold): the substep boundary folded into the first iteration's reads too
+  int gs_packed = 0;  // 1 (Gauss-Seidel, one CTA): the rows staged in shared memory in color order
 };
 
 // ---------------------------------------------------------------------------
@@ -308,11 +309,12 @@ XD void row_jacobi(Pos pos, const int4* ri, const float4* rf,
 XD void put3(float4* x, int i, V3 p) { x[i] = f4(p, x[i].w); }
 
 // kernels.py:105-208 solve_constraints_color, one row, in place.
-template <bool FIRST>
-XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, const float4* ra,
-               float* lam, int j, float h) {
-  int4 r = ri[j];
-  float lam_old = FIRST ? 0.0f : lam[j];
+// kernels.py:105-208 solve_constraints_color, one row, in place: the row's
+// record r, its parameters through fget() (read where the row's type needs
+// them), its ATTACH anchor, and its multiplier lam_old; returns the new one.
+template <class FGet>
+XD float row_gs_core(float4* x, const float4* xp, int4 r, FGet fget, const float4* anchor, float lam_old,
+                     float h) {
   float lam_new = lam_old;
   if (r.w != 0) {
     int t = r.x;
@@ -323,7 +325,7 @@ XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, co
       float wa = xa.w, wb;
       V3 pb;
       if (t == XPBD_ATTACH) {
-        pb = v3(ra[j]);
+        pb = v3(*anchor);
         wb = 0.0f;
       } else {
         float4 xb = x[r.z];
@@ -336,7 +338,7 @@ XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, co
         float L = length(d);
         if (!(L < kEps)) {
           V3 n_hat = d / L;
-          float4 f = rf[j];
+          float4 f = fget();
           float C = L - f.x;
           float alpha = f.y * inv_dt2;
           float dlam = (-C - alpha * lam_old) / (wsum + alpha);
@@ -350,7 +352,7 @@ XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, co
       float4 xa = x[a];
       float wa = xa.w;
       if (wa != 0.0f) {
-        float4 f = rf[j];
+        float4 f = fget();
         float C = xa.y - f.w;
         if (!(C >= 0.0f)) {
           float dlam = -C / wa;
@@ -374,7 +376,7 @@ XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, co
         float L = length(d);
         if (!(L < kEps)) {
           V3 n_hat = d / L;
-          float4 f = rf[j];
+          float4 f = fget();
           float C = L - f.x;
           if (!(C >= 0.0f)) {
             float dlam = -C / wsum;
@@ -395,7 +397,34 @@ XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, co
       }
     }
   }
+  return lam_new;
+}
+
+template <bool FIRST>
+XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, const float4* ra,
+               float* lam, int j, float h) {
+  const float lam_old = FIRST ? 0.0f : lam[j];
+  const float lam_new = row_gs_core(x, xp, ri[j], [&]() { return rf[j]; }, ra + j, lam_old, h);
   if (FIRST || lam_new != lam_old) lam[j] = lam_new;
+}
+
+// Gauss-Seidel rows staged in shared memory in color order (one-CTA driver):
+// int2 {a | type << 28 | active << 30, b (ATTACH: the row index, for its
+// anchor)} and the two parameters the row's type reads.
+constexpr int kPackTypeShift = 28;
+XD void pack_gs_row(int4 r, float4 f, int j, int2& pr, float2& pv) {
+  pr = make_int2(r.y | (r.x << kPackTypeShift) | ((r.w != 0 ? 1 : 0) << 30), r.x == XPBD_ATTACH ? j : r.z);
+  if (r.x == XPBD_FLOOR) pv = make_float2(f.z, f.w);
+  else if (r.x == XPBD_CONTACT) pv = make_float2(f.x, f.z);
+  else pv = make_float2(f.x, f.y);
+}
+XD void unpack_gs_row(int2 pr, float2 pv, int4& r, float4& f, int& j) {
+  const int t = (pr.x >> kPackTypeShift) & 3;
+  r = make_int4(t, pr.x & ((1 << kPackTypeShift) - 1), t == XPBD_ATTACH ? -1 : pr.y, (pr.x >> 30) & 1);
+  j = pr.y;
+  if (t == XPBD_FLOOR) f = make_float4(0.0f, 0.0f, pv.x, pv.y);
+  else if (t == XPBD_CONTACT) f = make_float4(pv.x, 0.0f, pv.y, 0.0f);
+  else f = make_float4(pv.x, pv.y, 0.0f, 0.0f);
 }
 
 struct AccGlobal {
@@ -458,6 +487,10 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
   asm volatile("griddepcontrol.wait;" ::: "memory");
   const int m = *g.n_rows;
   Dev3 s = g;
+  const bool packed = GS && SMEM && p.gs_packed;
+  int2* prow = nullptr;
+  float2* pval = nullptr;
+  int* cst = nullptr;
   if (SMEM) {
     s.x = smem;
     s.v = smem + n;
@@ -470,7 +503,26 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
       s.xp[i] = g.xp[i];
       s.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
-    for (int j = threadIdx.x; j < m; j += blockDim.x) s.lam[j] = g.lam[j];
+    if (packed) {
+      // rows, multipliers and color ranges in color order (the multipliers are
+      // written back by row index at the end)
+      prow = reinterpret_cast<int2*>(smem + 4 * n);
+      pval = reinterpret_cast<float2*>(prow + m);
+      s.lam = reinterpret_cast<float*>(pval + m);
+      cst = reinterpret_cast<int*>(s.lam + m);
+      for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        const int j = g.corder[k];
+        int2 pr;
+        float2 pv;
+        pack_gs_row(g.ri[j], g.rf[j], j, pr, pv);
+        prow[k] = pr;
+        pval[k] = pv;
+        s.lam[k] = g.lam[j];
+      }
+      for (int c = threadIdx.x; c <= g.ncolors; c += blockDim.x) cst[c] = g.cstarts[c];
+    } else {
+      for (int j = threadIdx.x; j < m; j += blockDim.x) s.lam[j] = g.lam[j];
+    }
     __syncthreads();
   }
   const V3 gv = V3{p.gx, p.gy, p.gz};
@@ -595,7 +647,23 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
       const bool more = (sub + 1 < p.substeps);  // integrate the next substep in this frame
       if (m > 0) {
         for (int it = 0; it < p.iterations; ++it) {
-          if (GS) {
+          if (GS && packed) {
+            for (int c = 0; c < g.ncolors; ++c) {
+              const int start = cst[c], count = cst[c + 1] - start;
+              for (int t = tid0; t < count; t += stride) {
+                const int k = start + t;
+                int4 r;
+                float4 f;
+                int jj;
+                unpack_gs_row(prow[k], pval[k], r, f, jj);
+                const float lam_old = it == 0 ? 0.0f : s.lam[k];
+                const float lam_new = row_gs_core(s.x, s.xp, r, [&]() { return f; },
+                                                  r.x == XPBD_ATTACH ? g.ra + jj : g.ra, lam_old, p.h);
+                if (it == 0 || lam_new != lam_old) s.lam[k] = lam_new;
+              }
+              sync();
+            }
+          } else if (GS) {
             for (int c = 0; c < g.ncolors; ++c) {
               int start = g.cstarts[c], count = g.cstarts[c + 1] - start;
               for (int t = tid0; t < count; t += stride) {
@@ -665,7 +733,11 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
       g.v[i] = s.v[i];
       g.xp[i] = s.xp[i];
     }
-    for (int j = threadIdx.x; j < m; j += blockDim.x) g.lam[j] = s.lam[j];
+    if (packed) {
+      for (int k = threadIdx.x; k < m; k += blockDim.x) g.lam[g.corder[k]] = s.lam[k];
+    } else {
+      for (int j = threadIdx.x; j < m; j += blockDim.x) g.lam[j] = s.lam[j];
+    }
   }
   if (cache_rows && p.iterations > 0) {
 #pragma unroll
@@ -955,11 +1027,24 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   if (mode == 1 && !fits) mode = 2;
   if (mode < 0) mode = fits ? 1 : (work <= 16LL * 1024 * 8 ? 2 : 0);
   h->mode = mode;
+  q.gs_packed = 0;
   if (mode == 1) {
     h->smem = smem;
     long long w = std::max<long long>(s->n_bodies, s->row_capacity / 4);
     h->threads = h->force_threads > 0 ? h->force_threads
                                       : (int)std::min<long long>(1024, std::max<long long>(128, ((w + 31) / 32) * 32));
+    // Gauss-Seidel: the rows too, in color order, when they fit (a phase then
+    // touches shared memory only)
+    if (p->gs && s->row_capacity > 0) {
+      size_t packed = (size_t)s->n_bodies * 4 * sizeof(float4) +
+                      (size_t)s->row_capacity * (sizeof(int2) + sizeof(float2) + sizeof(float)) +
+                      sizeof(int) * ((size_t)s->num_colors + 1);
+      packed = (packed + 15) & ~(size_t)15;
+      if (packed <= kSmemMax) {
+        q.gs_packed = 1;
+        h->smem = packed;
+      }
+    }
   } else {
     h->smem = 0;
     h->threads = h->force_threads > 0 ? std::min(h->force_threads, 512) : (mode == 2 ? 512 : 256);
