@@ -38,6 +38,11 @@ struct Dev3 {
   int ncolors;
   float4* accs = nullptr;  // folded Jacobi: per-iteration accumulators, then the carry buffers (handle memory)
   int acc_stride = 0;
+  // Gauss-Seidel on the cluster / grid drivers: the rows packed in color order
+  // at the start of every launch, and their multipliers (handle memory)
+  int2* gprow = nullptr;
+  float2* gpval = nullptr;
+  float* glam = nullptr;
 };
 
 struct Par3 {
@@ -45,7 +50,8 @@ struct Par3 {
   int cap_on, substeps, iterations, gs;
   int fold = 0;   // 1: Jacobi with the apply folded into the next iteration's reads
   int carry = 0;  // 1 (with fold): the substep boundary folded into the first iteration's reads too
-  int gs_packed = 0;  // 1 (Gauss-Seidel, one CTA): the rows staged in shared memory in color order
+  int gs_packed = 0;   // 1 (Gauss-Seidel, one CTA): the rows staged in shared memory in color order
+  int gs_gpacked = 0;  // 1 (Gauss-Seidel, cluster / grid): the rows packed in color order in global memory
 };
 
 // ---------------------------------------------------------------------------
@@ -311,24 +317,28 @@ XD void put3(float4* x, int i, V3 p) { x[i] = f4(p, x[i].w); }
 // kernels.py:105-208 solve_constraints_color, one row, in place.
 // kernels.py:105-208 solve_constraints_color, one row, in place: the row's
 // record r, its parameters through fget() (read where the row's type needs
-// them), its ATTACH anchor, and its multiplier lam_old; returns the new one.
+// them), its ATTACH anchor, its multiplier lam_old, and its endpoints' current
+// and substep-start positions, loaded by the caller (xb only for two-body
+// rows, xpa / xpb only where friction reads them); returns the new multiplier.
+// Rows of one color share no particle, so a caller may load the endpoints of
+// several rows of a color before projecting any of them.
+XD bool gs_uses_b(int t) { return t == XPBD_DISTANCE || t == XPBD_CONTACT; }
+XD bool gs_uses_xp(int t) { return t == XPBD_FLOOR || t == XPBD_CONTACT; }
 template <class FGet>
-XD float row_gs_core(float4* x, const float4* xp, int4 r, FGet fget, const float4* anchor, float lam_old,
-                     float h) {
+XD float row_gs_core(float4* x, int4 r, FGet fget, const float4* anchor, float lam_old, float h, float4 xa,
+                     float4 xb, float4 xpa, float4 xpb) {
   float lam_new = lam_old;
   if (r.w != 0) {
     int t = r.x;
     if (t == XPBD_DISTANCE || t == XPBD_ATTACH) {
       float inv_dt2 = 1.0f / (h * h);
       int a = r.y;
-      float4 xa = x[a];
       float wa = xa.w, wb;
       V3 pb;
       if (t == XPBD_ATTACH) {
         pb = v3(*anchor);
         wb = 0.0f;
       } else {
-        float4 xb = x[r.z];
         pb = v3(xb);
         wb = xb.w;
       }
@@ -343,13 +353,12 @@ XD float row_gs_core(float4* x, const float4* xp, int4 r, FGet fget, const float
           float alpha = f.y * inv_dt2;
           float dlam = (-C - alpha * lam_old) / (wsum + alpha);
           lam_new = lam_old + dlam;
-          put3(x, a, v3(xa) + n_hat * (wa * dlam));
-          if (t == XPBD_DISTANCE) put3(x, r.z, v3(x[r.z]) - n_hat * (wb * dlam));
+          x[a] = f4(v3(xa) + n_hat * (wa * dlam), xa.w);
+          if (t == XPBD_DISTANCE) x[r.z] = f4(v3(xb) - n_hat * (wb * dlam), xb.w);
         }
       }
     } else if (t == XPBD_FLOOR) {
       int a = r.y;
-      float4 xa = x[a];
       float wa = xa.w;
       if (wa != 0.0f) {
         float4 f = fget();
@@ -360,15 +369,14 @@ XD float row_gs_core(float4* x, const float4* xp, int4 r, FGet fget, const float
           V3 pa = v3(xa) + V3{0.0f, wa * dlam, 0.0f};
           float mu = f.z;
           if (mu > 0.0f) {
-            V3 dp_rel = pa - v3(xp[a]);
+            V3 dp_rel = pa - v3(xpa);
             pa = pa + friction_delta(dp_rel, V3{0.0f, 1.0f, 0.0f}, -C, mu);
           }
-          put3(x, a, pa);
+          x[a] = f4(pa, xa.w);
         }
       }
     } else if (t == XPBD_CONTACT) {
       int a = r.y, b = r.z;
-      float4 xa = x[a], xb = x[b];
       float wa = xa.w, wb = xb.w;
       float wsum = wa + wb;
       if (wsum != 0.0f) {
@@ -385,13 +393,13 @@ XD float row_gs_core(float4* x, const float4* xp, int4 r, FGet fget, const float
             V3 pb = v3(xb) - n_hat * (wb * dlam);
             float mu = f.z;
             if (mu > 0.0f) {
-              V3 dp_rel = (pa - v3(xp[a])) - (pb - v3(xp[b]));
+              V3 dp_rel = (pa - v3(xpa)) - (pb - v3(xpb));
               V3 corr = friction_delta(dp_rel, n_hat, -C, mu);
               pa = pa + corr * (wa / wsum);
               pb = pb - corr * (wb / wsum);
             }
-            put3(x, a, pa);
-            put3(x, b, pb);
+            x[a] = f4(pa, xa.w);
+            x[b] = f4(pb, xb.w);
           }
         }
       }
@@ -400,11 +408,27 @@ XD float row_gs_core(float4* x, const float4* xp, int4 r, FGet fget, const float
   return lam_new;
 }
 
+// The endpoints a row reads (nothing past the particle arrays for one-body rows).
+XD void gs_load_ends(const float4* x, const float4* xp, int4 r, float4& xa, float4& xb, float4& xpa,
+                     float4& xpb) {
+  const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  xa = x[r.y];
+  xb = gs_uses_b(r.x) ? x[r.z] : z;
+  xpa = gs_uses_xp(r.x) ? xp[r.y] : z;
+  xpb = r.x == XPBD_CONTACT ? xp[r.z] : z;
+}
+
 template <bool FIRST>
 XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, const float4* ra,
                float* lam, int j, float h) {
+  const int4 r = ri[j];
   const float lam_old = FIRST ? 0.0f : lam[j];
-  const float lam_new = row_gs_core(x, xp, ri[j], [&]() { return rf[j]; }, ra + j, lam_old, h);
+  float lam_new = lam_old;
+  if (r.w != 0) {
+    float4 xa, xb, xpa, xpb;
+    gs_load_ends(x, xp, r, xa, xb, xpa, xpb);
+    lam_new = row_gs_core(x, r, [&]() { return rf[j]; }, ra + j, lam_old, h, xa, xb, xpa, xpb);
+  }
   if (FIRST || lam_new != lam_old) lam[j] = lam_new;
 }
 
@@ -567,6 +591,19 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
   // has I barriers; the frame ends with one pass that applies, finalizes and
   // stores the frame state.
   const bool carry_path = !GS && !SMEM && p.fold && p.carry && m > 0;
+  const bool gpk = GS && !SMEM && p.gs_gpacked && m > 0;
+  if (gpk) {
+    for (int k = tid0; k < m; k += stride) {
+      const int j = g.corder[k];
+      int2 pr;
+      float2 pv;
+      pack_gs_row(g.ri[j], g.rf[j], j, pr, pv);
+      g.gprow[k] = pr;
+      g.gpval[k] = pv;
+      g.glam[k] = g.lam[j];
+    }
+    sync();
+  }
   auto rows_first = [&](const auto& pos, const AccGlobal& acc) {
     if (cache_rows) {
 #pragma unroll
@@ -657,9 +694,54 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
                 int jj;
                 unpack_gs_row(prow[k], pval[k], r, f, jj);
                 const float lam_old = it == 0 ? 0.0f : s.lam[k];
-                const float lam_new = row_gs_core(s.x, s.xp, r, [&]() { return f; },
-                                                  r.x == XPBD_ATTACH ? g.ra + jj : g.ra, lam_old, p.h);
+                float lam_new = lam_old;
+                if (r.w != 0) {
+                  float4 xa, xb, xpa, xpb;
+                  gs_load_ends(s.x, s.xp, r, xa, xb, xpa, xpb);
+                  lam_new = row_gs_core(s.x, r, [&]() { return f; }, r.x == XPBD_ATTACH ? g.ra + jj : g.ra, lam_old,
+                                        p.h, xa, xb, xpa, xpb);
+                }
                 if (it == 0 || lam_new != lam_old) s.lam[k] = lam_new;
+              }
+              sync();
+            }
+          } else if (GS && gpk) {
+            // two rows of the color per step: both records, then all their
+            // endpoints (rows of one color share no particle), then both projections
+            for (int c = 0; c < g.ncolors; ++c) {
+              const int start = g.cstarts[c], count = g.cstarts[c + 1] - start;
+              for (int t = tid0; t < count; t += 2 * stride) {
+                const int k0 = start + t, k1 = start + t + stride;
+                const bool has1 = t + stride < count;
+                const int2 pr0 = g.gprow[k0];
+                const float2 pv0 = g.gpval[k0];
+                const float lo0 = it == 0 ? 0.0f : g.glam[k0];
+                int2 pr1 = make_int2(0, 0);
+                float2 pv1 = make_float2(0.0f, 0.0f);
+                float lo1 = 0.0f;
+                if (has1) {
+                  pr1 = g.gprow[k1];
+                  pv1 = g.gpval[k1];
+                  lo1 = it == 0 ? 0.0f : g.glam[k1];
+                }
+                int4 r0, r1;
+                float4 f0, f1;
+                int j0, j1;
+                unpack_gs_row(pr0, pv0, r0, f0, j0);
+                unpack_gs_row(pr1, pv1, r1, f1, j1);
+                const bool on0 = r0.w != 0, on1 = has1 && r1.w != 0;
+                float4 xa0, xb0, xpa0, xpb0, xa1, xb1, xpa1, xpb1;
+                if (on0) gs_load_ends(s.x, s.xp, r0, xa0, xb0, xpa0, xpb0);
+                if (on1) gs_load_ends(s.x, s.xp, r1, xa1, xb1, xpa1, xpb1);
+                float ln0 = lo0, ln1 = lo1;
+                if (on0)
+                  ln0 = row_gs_core(s.x, r0, [&]() { return f0; }, r0.x == XPBD_ATTACH ? g.ra + j0 : g.ra, lo0, p.h,
+                                    xa0, xb0, xpa0, xpb0);
+                if (on1)
+                  ln1 = row_gs_core(s.x, r1, [&]() { return f1; }, r1.x == XPBD_ATTACH ? g.ra + j1 : g.ra, lo1, p.h,
+                                    xa1, xb1, xpa1, xpb1);
+                if (it == 0 || ln0 != lo0) g.glam[k0] = ln0;
+                if (has1 && (it == 0 || ln1 != lo1)) g.glam[k1] = ln1;
               }
               sync();
             }
@@ -738,6 +820,9 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
     } else {
       for (int j = threadIdx.x; j < m; j += blockDim.x) g.lam[j] = s.lam[j];
     }
+  }
+  if (gpk && p.iterations > 0) {
+    for (int k = tid0; k < m; k += stride) g.lam[g.corder[k]] = g.glam[k];
   }
   if (cache_rows && p.iterations > 0) {
 #pragma unroll
@@ -1074,6 +1159,27 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
     h->dev.acc_stride = s->n_bodies;
     q.fold = 1;
     q.carry = carry;
+  }
+  // Gauss-Seidel on the cluster / grid drivers: room for the rows packed in
+  // color order (the folded Jacobi buffers are never needed alongside)
+  q.gs_gpacked = 0;
+  h->dev.gprow = nullptr;
+  h->dev.gpval = nullptr;
+  h->dev.glam = nullptr;
+  if (p->gs && mode != 1 && s->row_capacity > 0) {
+    const size_t cap = (size_t)s->row_capacity;
+    const size_t bytes = cap * (sizeof(int2) + sizeof(float2) + sizeof(float));
+    if (bytes > h->accs_bytes) {
+      if (h->accs) cudaFree(h->accs);
+      h->accs = nullptr;
+      h->accs_bytes = 0;
+      XPBD_CUDA(cudaMalloc(&h->accs, bytes));
+      h->accs_bytes = bytes;
+    }
+    h->dev.gprow = reinterpret_cast<int2*>(h->accs);
+    h->dev.gpval = reinterpret_cast<float2*>(h->dev.gprow + cap);
+    h->dev.glam = reinterpret_cast<float*>(h->dev.gpval + cap);
+    q.gs_gpacked = 1;
   }
   int rc;
   if (p->gs) rc = mode == 1 ? configure<true, true>(h) : configure<true, false>(h);
