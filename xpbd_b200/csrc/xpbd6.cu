@@ -1381,21 +1381,21 @@ __global__ void k6_refit(int n, BP6 b, const int* scene, int* status) {
     int body = (int)b.vals[k];
     b.nlo[node] = b.lo[body];
     b.nhi[node] = b.hi[body];
-    __threadfence();
     int cur = b.parent[node];
     for (int depth = 0; cur >= 0; ++depth) {
       if (depth >= kMaxDepth || cur >= n - 1) {
         raise_status(status, XPBD_ERR_BAD_INDEX);
         break;
       }
-      if (atomicAdd(&b.flags[cur], 1) == 0) break;
-      __threadfence();
+      // acquire-release: the first walker's arrival releases the bounds it
+      // wrote; the second walker's arrival acquires them before it reads both
+      // children (one ordering atomic per level, no sequentially consistent fences)
+      if (atom_add_acq_rel_gpu(&b.flags[cur], 1) == 0) break;
       int2 c = b.child[cur];
       float4 l0 = __ldcg(b.nlo + c.x), l1 = __ldcg(b.nlo + c.y);
       float4 h0 = __ldcg(b.nhi + c.x), h1 = __ldcg(b.nhi + c.y);
       b.nlo[cur] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
       b.nhi[cur] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
-      __threadfence();
       cur = b.parent[cur];
     }
   }
