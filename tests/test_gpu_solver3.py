@@ -287,13 +287,15 @@ def test_contact_capacity_overflow_grows():
 def test_primitives_sort_and_scan():
     rng = np.random.default_rng(0)
     L = N.lib()
-    for n in (1, 5, 1000, 5000):
+    # one CTA up to 16384 keys, then tiles over many CTAs (8 passes for 64
+    # bits; 5 for 40 bits, which end in the scratch buffers and copy back)
+    for n, bits in ((1, 64), (5, 64), (1000, 64), (5000, 64), (20000, 64), (100000, 40), (70001, 64)):
         keys = rng.integers(0, 1 << 40, n, dtype=np.uint64)
         keys[: n // 3] = keys[0]  # ties keep input order
         vals = np.arange(n, dtype=np.uint32)
         tk = torch.from_numpy(keys.view(np.int64)).cuda()
         tv = torch.from_numpy(vals.view(np.int32)).cuda()
-        N.check(L.xpbd_sort_pairs_u64(N.ptr(tk), N.ptr(tv), n, 64, N.stream_of("cuda:0")))
+        N.check(L.xpbd_sort_pairs_u64(N.ptr(tk), N.ptr(tv), n, bits, N.stream_of("cuda:0")))
         order = np.argsort(keys, kind="stable")
         np.testing.assert_array_equal(tk.cpu().numpy().view(np.uint64), keys[order])
         np.testing.assert_array_equal(tv.cpu().numpy().view(np.uint32), vals[order])

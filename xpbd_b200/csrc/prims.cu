@@ -6,6 +6,8 @@
 // scan over the 32 warp histograms) and scattered.  Passes stop at the highest
 // set bit of the largest key, found on the device, so no host round trip is
 // needed.  The broad phases sort one key per body, which this covers.
+#include <utility>
+
 #include "prims.cuh"
 
 namespace xpbd {
@@ -18,14 +20,113 @@ __global__ void __launch_bounds__(1024) k_radix_sort_block(uint64_t* k0, uint32_
   block_sort_pairs_u64(S, k0, v0, k1, v1, n, max_bits);
 }
 
-size_t sort_scratch_bytes(int n) { return (size_t)(n > 0 ? n : 1) * (sizeof(uint64_t) + sizeof(uint32_t)) + 16; }
+// Above kSortMultiMin keys the passes are split over many CTAs, one tile of
+// kSortTile keys each: per 8-bit pass a per-tile digit histogram, an exclusive
+// scan of the digit-major counts (digit d of tile t at d * tiles + t), and a
+// stable scatter (each key's rank within its tile: in-warp rank from
+// __match_any_sync plus the counts of the same digit in earlier warps).  The
+// passes are ceil(max_bits / 8), planned on the host.
+constexpr int kSortMultiMin = 16384;
+constexpr int kSortTile = 1024;
+
+__global__ void __launch_bounds__(kSortTile) k_sort_hist(const uint64_t* in, int n, int shift, int tiles,
+                                                          int* hist) {
+  __shared__ int h[256];
+  if (threadIdx.x < 256) h[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * kSortTile + threadIdx.x;
+  if (i < n) atomicAdd(&h[(unsigned)((in[i] >> shift) & 255ull)], 1);
+  __syncthreads();
+  if (threadIdx.x < 256) hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kSortTile) k_sort_scatter(const uint64_t* kin, const uint32_t* vin, uint64_t* kout,
+                                                             uint32_t* vout, int n, int shift, int tiles,
+                                                             const int* offs) {
+  __shared__ unsigned wcnt[kSortTile / 32][257];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i = blockIdx.x * kSortTile + tid;
+  const bool valid = i < n;
+  const uint64_t key = valid ? kin[i] : 0ull;
+  const uint32_t val = valid ? vin[i] : 0u;
+  const unsigned d = valid ? (unsigned)((key >> shift) & 255ull) : 256u;
+  for (int q = tid; q < (kSortTile / 32) * 257; q += kSortTile) (&wcnt[0][0])[q] = 0u;
+  __syncthreads();
+  const unsigned peers = __match_any_sync(kFull, d);
+  const unsigned rank = __popc(peers & ((1u << lane) - 1u));
+  if (rank == 0) wcnt[warp][d] = __popc(peers);
+  __syncthreads();
+  if (tid < 256) {  // per digit: the counts of the earlier warps
+    unsigned run = 0;
+    for (int w = 0; w < kSortTile / 32; ++w) {
+      const unsigned c = wcnt[w][tid];
+      wcnt[w][tid] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  if (valid) {
+    const int pos = offs[d * tiles + blockIdx.x] + (int)wcnt[warp][d] + (int)rank;
+    kout[pos] = key;
+    vout[pos] = val;
+  }
+}
+
+__global__ void k_sort_copy(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, uint32_t* vout, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    kout[i] = kin[i];
+    vout[i] = vin[i];
+  }
+}
+
+size_t sort_scratch_bytes(int n) {
+  const size_t base = (size_t)(n > 0 ? n : 1) * (sizeof(uint64_t) + sizeof(uint32_t)) + 16;
+  if (n <= kSortMultiMin) return base;
+  const size_t counts = (size_t)256 * ceil_div(n, kSortTile);
+  const size_t align = 256;
+  return ((base + align - 1) / align) * align + 2 * ((counts * sizeof(int) + align - 1) / align) * align +
+         scan_scratch_bytes((int)counts) + align;
+}
 
 int sort_pairs_u64(uint64_t* keys, uint32_t* vals, int n, void* scratch, int max_bits, cudaStream_t stream) {
   if (n <= 1) return XPBD_OK;
   uint64_t* k1 = reinterpret_cast<uint64_t*>(scratch);
   uint32_t* v1 = reinterpret_cast<uint32_t*>(k1 + n);
-  k_radix_sort_block<<<1, 1024, 0, stream>>>(keys, vals, k1, v1, n, max_bits);
-  XPBD_LAUNCHED();
+  if (n <= kSortMultiMin) {
+    k_radix_sort_block<<<1, 1024, 0, stream>>>(keys, vals, k1, v1, n, max_bits);
+    XPBD_LAUNCHED();
+    return XPBD_OK;
+  }
+  const int tiles = ceil_div(n, kSortTile);
+  const size_t counts = (size_t)256 * tiles;
+  const size_t align = 256;
+  char* b = static_cast<char*>(scratch);
+  size_t off = (((size_t)n * (sizeof(uint64_t) + sizeof(uint32_t)) + 16 + align - 1) / align) * align;
+  int* hist = reinterpret_cast<int*>(b + off);
+  off += ((counts * sizeof(int) + align - 1) / align) * align;
+  int* offs = reinterpret_cast<int*>(b + off);
+  off += ((counts * sizeof(int) + align - 1) / align) * align;
+  void* scan_tmp = b + off;
+  off += scan_scratch_bytes((int)counts);
+  int* total = reinterpret_cast<int*>(b + off);
+  const int bits = max_bits < 1 ? 1 : (max_bits > 64 ? 64 : max_bits);
+  const int passes = (bits + 7) / 8;
+  uint64_t *ks = keys, *kd = k1;
+  uint32_t *vs = vals, *vd = v1;
+  for (int pass = 0; pass < passes; ++pass) {
+    k_sort_hist<<<tiles, kSortTile, 0, stream>>>(ks, n, 8 * pass, tiles, hist);
+    XPBD_LAUNCHED();
+    int rc = exclusive_scan_i32(hist, offs, (int)counts, total, scan_tmp, stream);
+    if (rc) return rc;
+    k_sort_scatter<<<tiles, kSortTile, 0, stream>>>(ks, vs, kd, vd, n, 8 * pass, tiles, offs);
+    XPBD_LAUNCHED();
+    std::swap(ks, kd);
+    std::swap(vs, vd);
+  }
+  if (ks != keys) {  // an odd number of passes ends in the scratch buffers
+    k_sort_copy<<<stream_blocks(n, 256), 256, 0, stream>>>(ks, vs, keys, vals, n);
+    XPBD_LAUNCHED();
+  }
   return XPBD_OK;
 }
 
