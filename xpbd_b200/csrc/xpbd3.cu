@@ -436,6 +436,7 @@ XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, co
 // int2 {a | type << 28 | active << 30, b (ATTACH: the row index, for its
 // anchor)} and the two parameters the row's type reads.
 constexpr int kPackTypeShift = 28;
+constexpr int kGsBatch = 4;  // rows per step of the packed global Gauss-Seidel loop
 XD void pack_gs_row(int4 r, float4 f, int j, int2& pr, float2& pv) {
   pr = make_int2(r.y | (r.x << kPackTypeShift) | ((r.w != 0 ? 1 : 0) << 30), r.x == XPBD_ATTACH ? j : r.z);
   if (r.x == XPBD_FLOOR) pv = make_float2(f.z, f.w);
@@ -706,42 +707,48 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
               sync();
             }
           } else if (GS && gpk) {
-            // two rows of the color per step: both records, then all their
-            // endpoints (rows of one color share no particle), then both projections
+            // kGsBatch rows of the color per step: their records, then all their
+            // endpoints (rows of one color share no particle), then the projections
             for (int c = 0; c < g.ncolors; ++c) {
               const int start = g.cstarts[c], count = g.cstarts[c + 1] - start;
-              for (int t = tid0; t < count; t += 2 * stride) {
-                const int k0 = start + t, k1 = start + t + stride;
-                const bool has1 = t + stride < count;
-                const int2 pr0 = g.gprow[k0];
-                const float2 pv0 = g.gpval[k0];
-                const float lo0 = it == 0 ? 0.0f : g.glam[k0];
-                int2 pr1 = make_int2(0, 0);
-                float2 pv1 = make_float2(0.0f, 0.0f);
-                float lo1 = 0.0f;
-                if (has1) {
-                  pr1 = g.gprow[k1];
-                  pv1 = g.gpval[k1];
-                  lo1 = it == 0 ? 0.0f : g.glam[k1];
+              for (int t = tid0; t < count; t += kGsBatch * stride) {
+                int2 pr[kGsBatch];
+                float2 pv[kGsBatch];
+                float lo[kGsBatch];
+#pragma unroll
+                for (int q = 0; q < kGsBatch; ++q) {
+                  const int tq = t + q * stride;
+                  pr[q] = make_int2(0, 0);
+                  pv[q] = make_float2(0.0f, 0.0f);
+                  lo[q] = 0.0f;
+                  if (tq < count) {
+                    pr[q] = g.gprow[start + tq];
+                    pv[q] = g.gpval[start + tq];
+                    if (it != 0) lo[q] = g.glam[start + tq];
+                  }
                 }
-                int4 r0, r1;
-                float4 f0, f1;
-                int j0, j1;
-                unpack_gs_row(pr0, pv0, r0, f0, j0);
-                unpack_gs_row(pr1, pv1, r1, f1, j1);
-                const bool on0 = r0.w != 0, on1 = has1 && r1.w != 0;
-                float4 xa0, xb0, xpa0, xpb0, xa1, xb1, xpa1, xpb1;
-                if (on0) gs_load_ends(s.x, s.xp, r0, xa0, xb0, xpa0, xpb0);
-                if (on1) gs_load_ends(s.x, s.xp, r1, xa1, xb1, xpa1, xpb1);
-                float ln0 = lo0, ln1 = lo1;
-                if (on0)
-                  ln0 = row_gs_core(s.x, r0, [&]() { return f0; }, r0.x == XPBD_ATTACH ? g.ra + j0 : g.ra, lo0, p.h,
-                                    xa0, xb0, xpa0, xpb0);
-                if (on1)
-                  ln1 = row_gs_core(s.x, r1, [&]() { return f1; }, r1.x == XPBD_ATTACH ? g.ra + j1 : g.ra, lo1, p.h,
-                                    xa1, xb1, xpa1, xpb1);
-                if (it == 0 || ln0 != lo0) g.glam[k0] = ln0;
-                if (has1 && (it == 0 || ln1 != lo1)) g.glam[k1] = ln1;
+                float4 xa[kGsBatch], xb[kGsBatch], xpa[kGsBatch], xpb[kGsBatch];
+#pragma unroll
+                for (int q = 0; q < kGsBatch; ++q) {
+                  int4 r;
+                  float4 f;
+                  int jj;
+                  unpack_gs_row(pr[q], pv[q], r, f, jj);
+                  if (r.w != 0) gs_load_ends(s.x, s.xp, r, xa[q], xb[q], xpa[q], xpb[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < kGsBatch; ++q) {
+                  const int tq = t + q * stride;
+                  int4 r;
+                  float4 f;
+                  int jj;
+                  unpack_gs_row(pr[q], pv[q], r, f, jj);
+                  float ln = lo[q];
+                  if (r.w != 0)
+                    ln = row_gs_core(s.x, r, [&]() { return f; }, r.x == XPBD_ATTACH ? g.ra + jj : g.ra, lo[q], p.h,
+                                     xa[q], xb[q], xpa[q], xpb[q]);
+                  if (tq < count && (it == 0 || ln != lo[q])) g.glam[start + tq] = ln;
+                }
               }
               sync();
             }
