@@ -372,3 +372,24 @@ def test_captured_frame_with_contacts_matches_host_driven_frames():
     sb.step()
     assert sb._hooked and sb.binds == binds + 1 and sb.launch_info()["mode"] == "grid"
     assert sb.status() == 0
+
+
+def test_gs_drivers_agree_on_attach_rows():
+    """The packed Gauss-Seidel rows keep an ATTACH row's index for its anchor:
+    the chain scene (distance rows, an ATTACH row, floor rows) gives the same
+    bits on the one-CTA, cluster and grid drivers."""
+    import make_golden as MG
+    res = {}
+    for drv in ((1, 0, 0), (2, 4, 256), (0, 0, 256)):
+        s = Solver(device="cuda:0", dt=1 / 60, substeps=10, iterations=2, solve_mode="gs")
+        MG.chain_scene(s)
+        s.set_driver(*drv)
+        for _ in range(3):
+            s.step()
+        assert s.status() == 0
+        res[drv] = (s.positions(), s.lambdas())
+    ref = res[(1, 0, 0)]
+    assert np.any(ref[1] != 0.0)
+    for drv, (x, lam) in res.items():
+        np.testing.assert_array_equal(x, ref[0])
+        np.testing.assert_array_equal(lam, ref[1])
