@@ -317,16 +317,18 @@ XD void put3(float4* x, int i, V3 p) { x[i] = f4(p, x[i].w); }
 // kernels.py:105-208 solve_constraints_color, one row, in place.
 // kernels.py:105-208 solve_constraints_color, one row, in place: the row's
 // record r, its parameters through fget() (read where the row's type needs
-// them), its ATTACH anchor, its multiplier lam_old, and its endpoints' current
-// and substep-start positions, loaded by the caller (xb only for two-body
-// rows, xpa / xpb only where friction reads them); returns the new multiplier.
-// Rows of one color share no particle, so a caller may load the endpoints of
-// several rows of a color before projecting any of them.
+// them), its ATTACH anchor, its multiplier lam_old, its endpoints' current
+// positions loaded by the caller (xb only for two-body rows), and their
+// substep-start positions through xpget(0) / xpget(1) (read only where
+// friction needs them: preloaded values on the latency-bound packed path, a
+// lazy read elsewhere); returns the new multiplier.  Rows of one color share
+// no particle, so a caller may load the endpoints of several rows of a color
+// before projecting any of them.
 XD bool gs_uses_b(int t) { return t == XPBD_DISTANCE || t == XPBD_CONTACT; }
 XD bool gs_uses_xp(int t) { return t == XPBD_FLOOR || t == XPBD_CONTACT; }
-template <class FGet>
-XD float row_gs_core(float4* x, int4 r, FGet fget, const float4* anchor, float lam_old, float h, float4 xa,
-                     float4 xb, float4 xpa, float4 xpb) {
+template <class FGet, class XPGet>
+XD float row_gs_core(float4* x, int4 r, FGet fget, XPGet xpget, const float4* anchor, float lam_old, float h,
+                     float4 xa, float4 xb) {
   float lam_new = lam_old;
   if (r.w != 0) {
     int t = r.x;
@@ -369,7 +371,7 @@ XD float row_gs_core(float4* x, int4 r, FGet fget, const float4* anchor, float l
           V3 pa = v3(xa) + V3{0.0f, wa * dlam, 0.0f};
           float mu = f.z;
           if (mu > 0.0f) {
-            V3 dp_rel = pa - v3(xpa);
+            V3 dp_rel = pa - v3(xpget(0));
             pa = pa + friction_delta(dp_rel, V3{0.0f, 1.0f, 0.0f}, -C, mu);
           }
           x[a] = f4(pa, xa.w);
@@ -393,7 +395,7 @@ XD float row_gs_core(float4* x, int4 r, FGet fget, const float4* anchor, float l
             V3 pb = v3(xb) - n_hat * (wb * dlam);
             float mu = f.z;
             if (mu > 0.0f) {
-              V3 dp_rel = (pa - v3(xpa)) - (pb - v3(xpb));
+              V3 dp_rel = (pa - v3(xpget(0))) - (pb - v3(xpget(1)));
               V3 corr = friction_delta(dp_rel, n_hat, -C, mu);
               pa = pa + corr * (wa / wsum);
               pb = pb - corr * (wb / wsum);
@@ -409,11 +411,14 @@ XD float row_gs_core(float4* x, int4 r, FGet fget, const float4* anchor, float l
 }
 
 // The endpoints a row reads (nothing past the particle arrays for one-body rows).
+XD void gs_load_x(const float4* x, int4 r, float4& xa, float4& xb) {
+  xa = x[r.y];
+  xb = gs_uses_b(r.x) ? x[r.z] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
 XD void gs_load_ends(const float4* x, const float4* xp, int4 r, float4& xa, float4& xb, float4& xpa,
                      float4& xpb) {
   const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  xa = x[r.y];
-  xb = gs_uses_b(r.x) ? x[r.z] : z;
+  gs_load_x(x, r, xa, xb);
   xpa = gs_uses_xp(r.x) ? xp[r.y] : z;
   xpb = r.x == XPBD_CONTACT ? xp[r.z] : z;
 }
@@ -425,9 +430,10 @@ XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, co
   const float lam_old = FIRST ? 0.0f : lam[j];
   float lam_new = lam_old;
   if (r.w != 0) {
-    float4 xa, xb, xpa, xpb;
-    gs_load_ends(x, xp, r, xa, xb, xpa, xpb);
-    lam_new = row_gs_core(x, r, [&]() { return rf[j]; }, ra + j, lam_old, h, xa, xb, xpa, xpb);
+    float4 xa, xb;
+    gs_load_x(x, r, xa, xb);
+    lam_new = row_gs_core(x, r, [&]() { return rf[j]; }, [&](int e) { return xp[e ? r.z : r.y]; }, ra + j,
+                          lam_old, h, xa, xb);
   }
   if (FIRST || lam_new != lam_old) lam[j] = lam_new;
 }
@@ -697,10 +703,10 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
                 const float lam_old = it == 0 ? 0.0f : s.lam[k];
                 float lam_new = lam_old;
                 if (r.w != 0) {
-                  float4 xa, xb, xpa, xpb;
-                  gs_load_ends(s.x, s.xp, r, xa, xb, xpa, xpb);
-                  lam_new = row_gs_core(s.x, r, [&]() { return f; }, r.x == XPBD_ATTACH ? g.ra + jj : g.ra, lam_old,
-                                        p.h, xa, xb, xpa, xpb);
+                  float4 xa, xb;
+                  gs_load_x(s.x, r, xa, xb);
+                  lam_new = row_gs_core(s.x, r, [&]() { return f; }, [&](int e) { return s.xp[e ? r.z : r.y]; },
+                                        r.x == XPBD_ATTACH ? g.ra + jj : g.ra, lam_old, p.h, xa, xb);
                 }
                 if (it == 0 || lam_new != lam_old) s.lam[k] = lam_new;
               }
@@ -745,8 +751,8 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
                   unpack_gs_row(pr[q], pv[q], r, f, jj);
                   float ln = lo[q];
                   if (r.w != 0)
-                    ln = row_gs_core(s.x, r, [&]() { return f; }, r.x == XPBD_ATTACH ? g.ra + jj : g.ra, lo[q], p.h,
-                                     xa[q], xb[q], xpa[q], xpb[q]);
+                    ln = row_gs_core(s.x, r, [&]() { return f; }, [&](int e) { return e ? xpb[q] : xpa[q]; },
+                                     r.x == XPBD_ATTACH ? g.ra + jj : g.ra, lo[q], p.h, xa[q], xb[q]);
                   if (tq < count && (it == 0 || ln != lo[q])) g.glam[start + tq] = ln;
                 }
               }
