@@ -46,6 +46,13 @@ extern "C" {
 const char* xpbd_version(void);
 /* Last CUDA error string recorded by a call that returned XPBD_ERR_CUDA. */
 const char* xpbd_last_error(void);
+/* Failure-detection self-test (no reference counterpart): a cooperative grid of
+ * `blocks` CTAs runs `rounds` of the engine's bounded grid barrier; CTA
+ * `absent` (-1: none) never arrives, so the others give up at the barrier's
+ * time limit (2 s) and set XPBD_ERR_BARRIER_TIMEOUT.  Writes the device status
+ * word to *status_out (host memory) and synchronizes the stream; the context
+ * stays usable. */
+int xpbd_barrier_selftest(int blocks, int absent, int rounds, int* status_out, void* stream);
 
 /* ========================================================================== */
 /* 3-DOF particle solver (replaces solver.py:57-508 + kernels.py)              */

@@ -100,3 +100,39 @@ extern "C" int xpbd_color_ranges(int m, const int* color, int* order, int* start
   for (int j = 0; j < m; ++j) order[cnt[color[j]]++] = j;
   return k;
 }
+
+// ---- failure detection self-test (no reference counterpart) ----------------------
+namespace xpbd {
+
+// `rounds` grid barriers; CTA `absent` (if >= 0) never arrives at them, so the
+// others give up at the barrier's time limit and raise the status bit.
+__global__ void k_barrier_selftest(GridBarrier b, int absent, int rounds) {
+  for (int r = 0; r < rounds; ++r)
+    if ((int)blockIdx.x != absent) grid_sync(b);
+  grid_exit(b);
+}
+
+}  // namespace xpbd
+
+extern "C" int xpbd_barrier_selftest(int blocks, int absent, int rounds, int* status_out, void* stream) {
+  using namespace xpbd;
+  if (blocks < 2 || absent >= blocks || rounds < 1 || rounds > 1000 || !status_out) return XPBD_ERR_BAD_ARG;
+  int per_sm = 0;
+  XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_barrier_selftest, 64, 0));
+  if (blocks > per_sm * num_sms()) return XPBD_ERR_BAD_ARG;  // a cooperative grid must be co-resident
+  cudaStream_t st = as_stream(stream);
+  unsigned* bar = nullptr;
+  XPBD_CUDA(cudaMalloc(&bar, 4 * sizeof(unsigned)));
+  cudaError_t e = cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), st);
+  GridBarrier gb = make_grid_barrier(bar, 0);
+  void* args[] = {&gb, &absent, &rounds};
+  if (e == cudaSuccess) e = cudaLaunchCooperativeKernel((void*)k_barrier_selftest, blocks, 64, args, 0, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(status_out, bar + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(bar);
+  if (e != cudaSuccess) {
+    set_last_error("xpbd_barrier_selftest", e);
+    return XPBD_ERR_CUDA;
+  }
+  return XPBD_OK;
+}
