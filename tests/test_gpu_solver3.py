@@ -96,15 +96,15 @@ def _disjoint_pairs(s):
 
 
 @pytest.mark.parametrize("drv", [(2, 4, 256), (0, 0, 256)], ids=["cluster", "grid"])
-@pytest.mark.parametrize("substeps", [15, 4])
-def test_folded_substeps_bit_exact_on_disjoint_pairs(drv, substeps):
+@pytest.mark.parametrize("substeps,iterations", [(15, 2), (4, 2), (5, 3), (4, 4)])
+def test_folded_substeps_bit_exact_on_disjoint_pairs(drv, substeps, iterations):
     """The folded drivers read each substep boundary on the fly (apply, finalize,
     clamp, integrate inside the first iteration's reads) and store the frame
     state in one closing pass.  Where atomic order cannot matter they match the
     oracle bit for bit: positions, velocities, substep-start positions and
     multipliers, after every frame (odd and even substep counts end in
-    different buffers)."""
-    kw = dict(dt=1 / 60, substeps=substeps, iterations=2, solve_mode="jacobi", damping=0.01, max_speed=3.0)
+    different buffers; two to four iterations, the folded range)."""
+    kw = dict(dt=1 / 60, substeps=substeps, iterations=iterations, solve_mode="jacobi", damping=0.01, max_speed=3.0)
     eng, orc = _pair(_disjoint_pairs, **kw)
     eng.set_driver(*drv)
     for f in range(4):
