@@ -1851,10 +1851,10 @@ __global__ void k6_red_init(BP6 b) {
   if (threadIdx.x >= 6 && threadIdx.x < 16) b.red[threadIdx.x] = 0;
 }
 
+// Row-major over the occupied cell box (the x extent only bounds the key).
 XD uint64_t cell_key(const int* red, int cx, int cy, int cz) {
-  uint64_t ex = (uint64_t)(red[3] - red[0] + 1), ey = (uint64_t)(red[4] - red[1] + 1);
-  (void)ex;
-  uint64_t ez = (uint64_t)(red[5] - red[2] + 1);
+  const uint64_t ey = (uint64_t)(red[4] - red[1] + 1);
+  const uint64_t ez = (uint64_t)(red[5] - red[2] + 1);
   return ((uint64_t)(cx - red[0]) * ey + (uint64_t)(cy - red[1])) * ez + (uint64_t)(cz - red[2]);
 }
 
