@@ -1535,6 +1535,7 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
   __shared__ BlockSortSmem sort_sm;
   __shared__ int s_bounds[6];
   __shared__ int s_scan[33];
+  __shared__ int s_fill[1024 / 8];  // per lane group: partners appended to its stage by the count walk
   const int n = s.n, tid = threadIdx.x, T = blockDim.x;
   const unsigned rank = cluster_rank(), csize = cluster_size();
   float4* LO = reinterpret_cast<float4*>(bp_dyn);
@@ -1554,6 +1555,7 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
     s_bounds[tid] = 0x7fffffff;
     s_bounds[3 + tid] = (int)0x80000000;
   }
+  if (tid < 1024 / 8) s_fill[tid] = 0;
   __syncthreads();
   // 1. kernels_bvh.py:22-48 body AABBs + bounds of their centres
   int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
@@ -1725,16 +1727,25 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
       my_start = -1;
     }
   }
-  auto count_body = [&](int i) {
-    int c = 0;
-    query_from(i, my_start, [&](int) { ++c; });
-    return c;
-  };
   // bodies interleaved over the cluster (i = rank + csize k), so the dense
   // parts of a scene spread over every CTA; the k-th body of this CTA goes to
   // group k mod NG
   const int mine_n = n > (int)rank ? (n - (int)rank + (int)csize - 1) / (int)csize : 0;
   const int gper = (mine_n + NG - 1) / NG;  // the same for every group of the CTA
+  // One body per group (always, up to kFusedMaxBoxes): the count walk also
+  // appends the partners to the group's stage (any order: the write pass
+  // sorts them), so a body whose pairs fit is written without a second walk.
+  auto count_body = [&](int i) {
+    int c = 0;
+    query_from(i, my_start, [&](int j) {
+      if (gper == 1) {
+        const int slot = atomicAdd(&s_fill[G], 1);
+        if (slot < kStagePairs) stage_all[G * kStagePairs + slot] = j;
+      }
+      ++c;
+    });
+    return c;
+  };
   auto body_of = [&](int k) { return (int)rank + (int)csize * (G + NG * k); };
   int saved[kMaxGroupBodies];  // this lane's count per body (registers: the loop is unrolled)
 #pragma unroll
@@ -1783,7 +1794,8 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
       ex -= c;
       const int base = live ? offs[i] : 0;
       const bool staged = body_total <= kStagePairs;
-      if (live && c > 0) {
+      const bool prestaged = staged && gper == 1;  // the count walk filled the stage already
+      if (live && c > 0 && !prestaged) {
         int r = 0;
         query_from(i, my_start, [&](int j) {
           if (staged) stage[ex + r] = j;
