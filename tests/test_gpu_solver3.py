@@ -393,3 +393,18 @@ def test_gs_drivers_agree_on_attach_rows():
     for drv, (x, lam) in res.items():
         np.testing.assert_array_equal(x, ref[0])
         np.testing.assert_array_equal(lam, ref[1])
+
+
+def test_captured_frame_reports_contact_overflow():
+    """Without the per-frame host check the captured frame cannot grow the
+    contact capacity: it keeps the rows that fit and raises XPBD_ERR_OVERFLOW in
+    the status word instead."""
+    s = Solver(device="cuda:0", dt=1 / 60, substeps=4, iterations=1, solve_mode="jacobi")
+    scenes.build_sphere_pile(s, nx=6, ny=6, nz=6, pitch=0.06, y0=0.3, jitter=0.0)
+    s.contact_capacity_per_body = 0  # the minimum capacity of 1024 rows
+    s.sync_contacts = False
+    s.step()
+    assert s._hooked
+    assert s.status() & N.XPBD_ERR_OVERFLOW
+    assert s.num_constraints == len(s.rows()["type"]) <= s._cap
+    assert np.all(np.isfinite(s.positions()))
