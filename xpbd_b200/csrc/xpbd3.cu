@@ -438,9 +438,10 @@ XD void row_gs(float4* x, const float4* xp, const int4* ri, const float4* rf, co
   if (FIRST || lam_new != lam_old) lam[j] = lam_new;
 }
 
-// Gauss-Seidel rows staged in shared memory in color order (one-CTA driver):
-// int2 {a | type << 28 | active << 30, b (ATTACH: the row index, for its
-// anchor)} and the two parameters the row's type reads.
+// Gauss-Seidel rows packed in color order (one-CTA driver: in shared memory;
+// cluster / grid drivers: in handle memory): int2 {a | type << 28 | active <<
+// 30, b (ATTACH: the row index, for its anchor)} and the two parameters the
+// row's type reads.  Scenes of 2^28 particles or more keep the unpacked rows.
 constexpr int kPackTypeShift = 28;
 constexpr int kGsBatch = 4;  // rows per step of the packed global Gauss-Seidel loop
 XD void pack_gs_row(int4 r, float4 f, int j, int2& pr, float2& pv) {
@@ -1133,7 +1134,7 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
                                       : (int)std::min<long long>(1024, std::max<long long>(128, ((w + 31) / 32) * 32));
     // Gauss-Seidel: the rows too, in color order, when they fit (a phase then
     // touches shared memory only)
-    if (p->gs && s->row_capacity > 0) {
+    if (p->gs && s->row_capacity > 0 && s->n_bodies < (1 << kPackTypeShift)) {
       size_t packed = (size_t)s->n_bodies * 4 * sizeof(float4) +
                       (size_t)s->row_capacity * (sizeof(int2) + sizeof(float2) + sizeof(float)) +
                       sizeof(int) * ((size_t)s->num_colors + 1);
@@ -1179,7 +1180,7 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   h->dev.gprow = nullptr;
   h->dev.gpval = nullptr;
   h->dev.glam = nullptr;
-  if (p->gs && mode != 1 && s->row_capacity > 0) {
+  if (p->gs && mode != 1 && s->row_capacity > 0 && s->n_bodies < (1 << kPackTypeShift)) {
     const size_t cap = (size_t)s->row_capacity;
     const size_t bytes = cap * (sizeof(int2) + sizeof(float2) + sizeof(float));
     if (bytes > h->accs_bytes) {
