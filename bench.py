@@ -147,6 +147,28 @@ def algorithmic_bytes(solver, rows_type_counts, gs):
     return b
 
 
+def lbvh_sort_launches(n, n_scenes):
+    """Kernel launches of the LBVH key sort (prims.cu sort_pairs_u64): one CTA up
+    to 16384 keys; above, per 8-bit pass a histogram, a 3-kernel scan and a
+    scatter, plus a copy back after an odd number of passes.  The keys carry 30
+    Morton bits plus the bits of the largest scene id."""
+    bits, ns = 30, n_scenes - 1
+    while ns > 0:
+        bits += 1
+        ns >>= 1
+    if n <= 16384:
+        return 1
+    passes = (bits + 7) // 8
+    return 5 * passes + passes % 2
+
+
+def batch_launches_per_frame(b):
+    """One frame kernel for the cloths; for the piles the multi-kernel LBVH chain
+    (init, AABB, Morton, sort, build, refit, count, 3-kernel scan, write) and one
+    substep kernel."""
+    return 1 + 10 + lbvh_sort_launches(b.piles.num_bodies, b.piles.n_scenes) + 1
+
+
 def time_batch(args, device, flush_buf, clocks=None, n_scenes=256, sample=(0, 1, 2, 3)):
     """Aggregate projections/s of the batched scenes, plus per-scene residual
     against the same scenes solved alone (a sample of scenes)."""
@@ -198,7 +220,7 @@ def time_batch(args, device, flush_buf, clocks=None, n_scenes=256, sample=(0, 1,
                 rows=rows3, bodies=n3 + n6, status=b.piles.status() | b.cloth.status(), alg_bytes=alg3 + alg6,
                 # cloth frame 1 + piles: multi-kernel LBVH (init, aabb, morton, sort, build,
                 # refit, count, scan (3), write) + substeps 1
-                launches=args.steps * 13,
+                launches=args.steps * batch_launches_per_frame(b),
                 launch={"cloth": b.cloth.launch_info(), "piles": b.piles.launch_info(), "autotune": tune,
                         "build_s": round(build_s, 1), "residual_max": float(res.max()),
                         "residual_median": float(np.median(res)), "vs_solo": checks,

@@ -46,3 +46,20 @@ def test_no_driver_runs_the_autotuner():
     rep = bench.pin_or_tune(s, argparse.Namespace(driver=""))
     assert s.calls == [("autotune", 3)]
     assert rep == {"ms_per_frame": {"x": 1.0}}
+
+
+def test_batch_launch_claim_counts_the_sort_passes():
+    """74,138 pile bodies in 128 scenes: 37-bit keys, five sort passes of five
+    launches plus the copy back, beside the eleven other pile kernels and the
+    cloths' frame kernel."""
+    assert bench.lbvh_sort_launches(1440, 1) == 1
+    assert bench.lbvh_sort_launches(74138, 128) == 26
+
+    class _Piles:
+        num_bodies = 74138
+        n_scenes = 128
+
+    class _Batch:
+        piles = _Piles()
+
+    assert bench.batch_launches_per_frame(_Batch()) == 38
