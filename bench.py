@@ -147,19 +147,23 @@ def algorithmic_bytes(solver, rows_type_counts, gs):
     return b
 
 
-def lbvh_sort_launches(n, n_scenes):
-    """Kernel launches of the LBVH key sort (prims.cu sort_pairs_u64): one CTA up
-    to 16384 keys; above, per 8-bit pass a histogram, a 3-kernel scan and a
-    scatter, plus a copy back after an odd number of passes.  The keys carry 30
-    Morton bits plus the bits of the largest scene id."""
-    bits, ns = 30, n_scenes - 1
-    while ns > 0:
-        bits += 1
-        ns >>= 1
+def sort_launches(n, bits):
+    """Kernel launches of prims.cu sort_pairs_u64: one CTA up to 16384 keys;
+    above, per 8-bit pass a histogram, a 3-kernel scan and a scatter, plus a copy
+    back after an odd number of passes."""
     if n <= 16384:
         return 1
     passes = (bits + 7) // 8
     return 5 * passes + passes % 2
+
+
+def lbvh_sort_launches(n, n_scenes):
+    """The LBVH key sort: 30 Morton bits plus the bits of the largest scene id."""
+    bits, ns = 30, n_scenes - 1
+    while ns > 0:
+        bits += 1
+        ns >>= 1
+    return sort_launches(n, bits)
 
 
 def batch_launches_per_frame(b):
@@ -248,9 +252,11 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
     stream = torch.cuda.current_stream(device)
     sp = C.c_void_p(stream.cuda_stream)
     # frame kernel + contact build: one fused cluster launch up to 4096 collidable
-    # spheres, else init, sanitize, cells, keys, sort, count, scan (3), write
+    # spheres, else init, sanitize, cells, keys, sort (63-bit cell keys), count,
+    # scan (3), write
     n_coll = int(s.tensors["collide_idx"].numel()) if s._self_collision else 0
-    launches_per_frame = 1 + ((1 if n_coll <= 4096 else 10) if s._self_collision else 0)
+    contact_launches = 1 if n_coll <= 4096 else 9 + sort_launches(n_coll, 63)
+    launches_per_frame = 1 + (contact_launches if s._self_collision else 0)
 
     s._flush()
     for _ in range(args.warmup):

@@ -63,3 +63,9 @@ def test_batch_launch_claim_counts_the_sort_passes():
         piles = _Piles()
 
     assert bench.batch_launches_per_frame(_Batch()) == 38
+
+
+def test_sort_launches_by_size_and_bits():
+    assert bench.sort_launches(16384, 63) == 1
+    assert bench.sort_launches(16385, 63) == 40  # eight passes, even: no copy back
+    assert bench.sort_launches(100000, 40) == 26  # five passes and the copy back
