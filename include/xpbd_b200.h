@@ -167,11 +167,12 @@ int xpbd3_attach_contacts(xpbd3_solver* h, xpbd3_contacts* c, const float* radiu
  * for callers that cannot allocate device memory while they step (a plugin
  * whose host owns all GPU allocations, or a fixed-budget simulation thread for
  * which cudaMalloc's device-wide synchronisation is off limits): all working
- * memory comes from one fixed device array inside the library (about 1.4 MB,
+ * memory comes from one fixed device array inside the library (about 1.3 MB,
  * held on every GPU that loads the library until exit) and the call performs
- * no allocation.  At most 8192 collidable spheres; larger n_collide returns
- * XPBD_ERR_BAD_ARG.  The first call on a device looks the array's address up
- * (make it before any stream capture).  All calls on a device share the array:
+ * no allocation.  At most 8192 collidable spheres (and no more than
+ * s->n_bodies); larger n_collide returns XPBD_ERR_BAD_ARG.  The first call on
+ * a device looks the array's address up (make it before any stream capture);
+ * the address is not valid after a device reset in the same process.  All calls on a device share the array:
  * calls on one stream run back to back safely, calls that overlap on the GPU
  * race and must be serialised by the caller. */
 int xpbd3_contacts_build_noalloc(const xpbd3_state* s, const float* radius, const float* friction,

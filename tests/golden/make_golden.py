@@ -1,10 +1,11 @@
 """Generate the golden fixtures in this folder by running the REFERENCE package
-(nanli9/XPBD ``src/xpbd3d``, read from ``/root/reference``) on the CPU through
+(nanli9/XPBD ``src/xpbd3d``, from a checkout of the reference project) on the CPU through
 ``warp_shim`` (a sequential stand-in for the Warp builtins it calls).
 
 Run once in a container that has the reference checked out:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>
+    XPBD_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 Nothing at test time reads the reference; the tests only read the ``.npz`` files
 this script writes.  Every fixture records the scene parameters, the initial
@@ -323,9 +324,12 @@ def host_fixtures(ref, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("XPBD_REFERENCE"),
+                    help="root of the reference checkout (default: $XPBD_REFERENCE)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or XPBD_REFERENCE")
     ref = load_reference(args.ref)
     out = {}
     jobs = {

@@ -744,11 +744,15 @@ extern "C" int xpbd3_contacts_build(xpbd3_contacts* c, const xpbd3_state* st, co
 // Limits and rules:
 //  * at most kNoAllocMaxCollide collidable spheres (8192); larger inputs are
 //    rejected with XPBD_ERR_BAD_ARG before anything is launched;
-//  * the array (about 1.4 MB) lives on every GPU that loads the library until
-//    the process exits;
+//  * the array (NoAllocLayout::bytes, about 1.3 MB) lives on every GPU that
+//    loads the library until the process exits;
 //  * the first call on a device looks the array's device address up with
 //    cudaGetSymbolAddress (with that device current) and caches it per device;
-//    make that first call before any stream capture begins;
+//    make that first call before any stream capture begins.  The cached
+//    address belongs to the device's primary context: after cudaDeviceReset
+//    (or anything else that destroys that context) the module is loaded again
+//    and the address is stale, so this entry point must not be used after a
+//    device reset in the same process;
 //  * every call on a device shares the one array and each call re-initialises
 //    what it needs (reductions, counts, offsets and totals are rewritten before
 //    they are read), so back-to-back calls on one stream are fine but calls
@@ -806,7 +810,8 @@ extern "C" int xpbd3_contacts_build_noalloc(const xpbd3_state* st, const float* 
                                             const int* collide_idx, int n_collide, const int64_t* existing,
                                             int n_existing, const float* x_init, double contact_margin,
                                             double dt, double r_max, int* status_dev, void* stream) {
-  if (!st || n_collide < 0 || n_collide > kNoAllocMaxCollide || !x_init || !radius || !friction ||
+  if (!st || n_collide < 0 || n_collide > kNoAllocMaxCollide || n_collide > st->n_bodies || !x_init ||
+      !radius || !friction ||
       (n_collide > 0 && !collide_idx) || (n_existing > 0 && !existing) || !st->n_rows)
     return XPBD_ERR_BAD_ARG;
   // sort_scratch_bytes / scan_scratch_bytes of the largest accepted input must fit the layout
