@@ -1,16 +1,19 @@
 #!/usr/bin/env python
 """Benchmark of the XPBD substep engine on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload spheres|cloth]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload boxes|spheres|cloth|cloth_jacobi|batch]
     python bench.py --impl reference ...      # the CPU restatement of the reference, timed on the host
 
 A step is one frame (dt = 1/60 s, 15 substeps x 2 iterations) of the workload.
-Default workload: the 2048-sphere pile (16 x 8 x 16 jittered lattice, r = 0.05 m,
-FLOOR rows, sphere-sphere self collision regenerated every frame, Jacobi).  The
-metric is constraint projections per second (rows x substeps x iterations per
-frame, the reference's benchmark definition, examples/benchmark.py:126) and
-ms/frame.  Multi-GPU runs are independent replicas (one scene per rank, no data
-exchange): value = sum over ranks of projections / max over ranks of time.
+Default workload: the 1440-box pile (12 x 10 x 12 lattice, pitch 0.8 m, half
+extents U[0.1, 0.3] m, random orientations, mu = 0.6, e = 0.2, LBVH broad phase),
+timed after 60 settling frames.  The metric is constraint projections per second
+(rows x substeps x iterations, the reference's benchmark definition,
+examples/benchmark.py:126; for 6-DOF rows = 8 floor slots per dynamic body +
+manifold points + joints per substep, the points counted on the device every
+substep) and ms/frame.  Multi-GPU runs are independent replicas of one scene (no
+data exchange), except the batch, whose scenes are split across the ranks by LPT
+bin packing: value = sum over ranks of projections / max over ranks of time.
 
 Timing: W untimed frames, then K frames each bracketed by CUDA events on the
 solver's stream, with the 126 MB L2 flushed (256 MB memset) between frames
@@ -21,7 +24,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -33,11 +35,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
+    "boxes": "box pile 1440 (12x10x12 lattice pitch 0.8 m, half extents U[0.1,0.3] m, density 1000, random "
+             "orientation, mu=0.6, e=0.2), LBVH, 15x2",
     "spheres": "sphere pile 2048 (16x8x16, r=0.05 m, jitter 0.01, floor + self collision mu=0.5), jacobi 15x2",
     "cloth": "cloth 32x32 (spacing 0.02 m, 0.01 kg, 2 pinned corners, 5826 DISTANCE alpha=1e-8 + 1024 FLOOR mu=0.3), gs 15x2",
     "cloth_jacobi": "cloth 32x32 as above, jacobi 15x2",
-    "boxes": "box pile 1440 (12x10x12 lattice pitch 0.8 m, half extents U[0.1,0.3] m, density 1000, random "
-             "orientation, mu=0.6, e=0.2), LBVH, 15x2",
     "batch": "256 independent scenes from seed 0: 128 cloths n x n (n ~ U{16..128}, gs, per-scene coloring) + "
              "128 box piles of k boxes (k ~ U{64..1024}, LBVH), packed into one 3-DOF and one 6-DOF system, 15x2",
 }
@@ -50,6 +52,9 @@ BYTES_PER_PROJ = {0: 88, 1: 88, 2: 64, 3: 112}   # DISTANCE, ATTACH, FLOOR, CONT
 BYTES_PER_PROJ_GS = {0: 84, 1: 84, 2: 64, 3: 112}
 APPLY_BYTES = 60          # per body per iteration (Jacobi averaged apply)
 BODY_SUBSTEP_BYTES = 128  # per body per substep (integrate + finalize + clamp)
+# 6-DOF per unit: manifold point projection, floor corner, joint, manifold
+# generation per pair per substep, body per substep
+POINT_BYTES, CORNER_BYTES, JOINT_BYTES, PAIR_GEN_BYTES, BODY6_BYTES = 196, 47, 196, 300, 128
 
 
 def make_solver(workload, device, solver_cls):
@@ -147,6 +152,12 @@ def algorithmic_bytes(solver, rows_type_counts, gs):
     return b
 
 
+def algorithmic_bytes6(S, I, n, n_dyn, n_joints, points_per_substep, pairs):
+    """Bytes of one frame of the 6-DOF substep kernel by the per-unit model."""
+    return int(S * (I * (points_per_substep * POINT_BYTES + 8 * n_dyn * CORNER_BYTES + n_joints * JOINT_BYTES)
+                    + pairs * PAIR_GEN_BYTES + n * BODY6_BYTES))
+
+
 def sort_launches(n, bits):
     """Kernel launches of prims.cu sort_pairs_u64: one CTA up to 16384 keys;
     above, per 8-bit pass a histogram, a 3-kernel scan and a scatter, plus a copy
@@ -170,25 +181,67 @@ def batch_launches_per_frame(b):
     """One frame kernel for the cloths; for the piles the multi-kernel LBVH chain
     (init, AABB, Morton, sort, build, refit, count, 3-kernel scan, write) and one
     substep kernel."""
-    return 1 + 10 + lbvh_sort_launches(b.piles.num_bodies, b.piles.n_scenes) + 1
+    n = 0
+    if getattr(b, "has_cloth", True):
+        n += 1
+    if getattr(b, "has_piles", True):
+        n += 10 + lbvh_sort_launches(b.piles.num_bodies, b.piles.n_scenes) + 1
+    return n
 
 
-def time_batch(args, device, flush_buf, clocks=None, n_scenes=256, sample=(0, 1, 2, 3)):
-    """Aggregate projections/s of the batched scenes, plus per-scene residual
-    against the same scenes solved alone (a sample of scenes)."""
+def phase_floor_us(launch, device, rounds=2000, repeats=3):
+    """Measured latency floor of one phase on the driver of `launch` (mode,
+    blocks, threads): xpbd_phase_floor's dependent L2 load + vector reduction +
+    barrier, median of `repeats` runs of `rounds` phases."""
+    import ctypes as C
+
+    from xpbd_b200 import _native as N
+    mode = {"grid": 0, "shared": 1, "cluster": 2}[launch["mode"]]
+    vals = []
+    for _ in range(repeats):
+        ns = C.c_float(0.0)
+        N.check(N.lib().xpbd_phase_floor(mode, int(launch["blocks"]), int(launch["threads"]), rounds,
+                                         C.byref(ns), N.stream_of(device)), "xpbd_phase_floor")
+        vals.append(ns.value / 1e3)
+    return statistics.median(vals)
+
+
+def latency_model(kernel, kern_ms, barriers, phases, launch, device):
+    """Frame kernel time against the phase latency floor: a frame of a scene
+    this small is a chain of `phases` dependent phases, each at least one
+    barrier plus one dependent L2 round trip."""
+    floor = phase_floor_us(launch, device)
+    us = kern_ms * 1e3 / max(phases, 1)
+    return {"kernel": kernel, "barriers_per_frame": barriers, "phases_per_frame": phases,
+            "us_per_phase": round(us, 4), "floor_us_per_phase": round(floor, 4), "frac": round(floor / us, 4),
+            "floor_probe": f"{launch['mode']} {launch['blocks']}x{launch['threads']}: one dependent L2 load + "
+                           "one vector reduction + the barrier per phase (xpbd_phase_floor)"}
+
+
+def time_batch(args, device, flush_buf, clocks=None, rank=0, world=1, n_scenes=256, sample=(0, 1, 2, 3)):
+    """Aggregate projections/s of the batched scenes (this rank's share when the
+    batch is sharded), plus per-scene residual against the same scenes solved
+    alone (a sample of this rank's scenes)."""
     import numpy as np
     import torch
 
-    from xpbd_b200.batch import BatchedScenes, batch_specs
+    from xpbd_b200.batch import BatchedScenes, batch_specs, rank_scene_ids
+    from xpbd_b200.shard import gather_scene_metrics
+    specs = batch_specs(n_scenes, seed=0)
+    ids = rank_scene_ids(specs, rank, world)
     t0 = time.perf_counter()
-    b = BatchedScenes(batch_specs(n_scenes, seed=0), device=device)
+    b = BatchedScenes(specs, device=device, scene_ids=ids)
     build_s = time.perf_counter() - t0
     for _ in range(args.warmup):
         b.step()
     tune = b.autotune(frames=2)  # on the warmed-up state (contacts present), restored afterwards
     torch.cuda.synchronize(device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     stream = torch.cuda.current_stream(device)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    b.reset_projection_count()
     ctx = clocks if clocks is not None else _Null()
     with ctx:
         for k in range(args.steps):
@@ -199,11 +252,30 @@ def time_batch(args, device, flush_buf, clocks=None, n_scenes=256, sample=(0, 1,
             ev[k][1].record(stream)
         torch.cuda.synchronize(device)
     frame_ms = [a.elapsed_time(c) for a, c in ev]
-    proj = b.projections_per_frame()
+    proj_total = b.projections(args.steps)
+    points_total = b.piles.manifold_points() if b.has_piles else 0
     res = b.residuals()
     frames_done = args.warmup + args.steps
+    # per-kernel time on further frames (each system alone, L2 flushed), for the roofline
+    S, I = b.cloth.substeps, b.cloth.iterations
+    kern = {}
+    for name, sys_, on in (("cloth", b.cloth, b.has_cloth), ("piles", b.piles, b.has_piles)):
+        if not on:
+            continue
+        kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(5)]
+        for e1, e2 in kev:
+            if flush_buf is not None:
+                flush_buf.zero_()
+            e1.record(stream)
+            sys_.step()
+            e2.record(stream)
+        torch.cuda.synchronize(device)
+        kern[name] = statistics.mean(a.elapsed_time(c) for a, c in kev)
+    frames_done += 5
     checks = {}
     for i in sample:
+        if i not in b.scene_ids:
+            continue
         s = b.solo(i)
         for _ in range(frames_done):
             s.step()
@@ -211,32 +283,47 @@ def time_batch(args, device, flush_buf, clocks=None, n_scenes=256, sample=(0, 1,
         d = float(np.abs(b.scene_positions(i) - s.positions()).max())
         checks[str(i)] = {"kind": b.specs[i].kind, "size": b.specs[i].size, "residual_batched": float(res[i]),
                           "residual_solo": float(s.residual()[0]), "max_abs_dx_vs_solo": d}
-    S, I = b.cloth.substeps, b.cloth.iterations
-    rows3 = b.cloth.num_constraints
-    n3 = b.cloth.num_bodies
-    alg3 = S * I * rows3 * 84 + S * n3 * BODY_SUBSTEP_BYTES
-    T = b.piles.tensors
-    npairs = min(b.piles.n_pairs, b.piles.cap)
-    pts = int(T["m_hdr"][:npairs, 0].sum().item())
-    n6 = b.piles.num_bodies
-    alg6 = S * (I * (pts * 196 + 8 * n6 * 47) + npairs * 300 + n6 * 128)
-    return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=frame_ms, proj_per_frame=proj,
-                rows=rows3, bodies=n3 + n6, status=b.piles.status() | b.cloth.status(), alg_bytes=alg3 + alg6,
-                # cloth frame 1 + piles: multi-kernel LBVH (init, aabb, morton, sort, build,
-                # refit, count, scan (3), write) + substeps 1
-                launches=args.steps * batch_launches_per_frame(b),
-                launch={"cloth": b.cloth.launch_info(), "piles": b.piles.launch_info(), "autotune": tune,
-                        "build_s": round(build_s, 1), "residual_max": float(res.max()),
-                        "residual_median": float(np.median(res)), "vs_solo": checks,
+    rows3 = b.cloth.num_constraints if b.has_cloth else 0
+    n3 = b.cloth.num_bodies if b.has_cloth else 0
+    alg3 = S * I * rows3 * BYTES_PER_PROJ_GS[0] + S * n3 * BODY_SUBSTEP_BYTES
+    npairs, n6, alg6 = 0, 0, 0
+    if b.has_piles:
+        T = b.piles.tensors
+        npairs = min(b.piles.n_pairs, b.piles.cap)
+        n6 = b.piles.num_bodies
+        n_dyn6 = int((T["x"][:, 3] > 0).sum().item())
+        alg6 = algorithmic_bytes6(S, I, n6, n_dyn6, b.piles.num_joints, points_total / (args.steps * S), npairs)
+    # every scene's residual, whichever rank stepped it
+    held = [i for i in b.scene_ids]
+    all_res = gather_scene_metrics(held, [float(res[i]) for i in held], len(specs))
+    hbm, _ = peaks()
+    rl = {}
+    for name, alg in (("cloth", alg3), ("piles", alg6)):
+        if name in kern:
+            ach = alg / (kern[name] / 1e3) / 1e9
+            rl[name] = {"kernel": "k3_frames (gs, grid)" if name == "cloth" else "LBVH chain + k6_substeps",
+                        "alg_bytes_per_frame": int(alg), "ms": round(kern[name], 5), "achieved_gbs": round(ach, 1),
+                        "frac": round(ach / hbm, 4)}
+    return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=frame_ms, proj_total=proj_total,
+                rows=rows3, bodies=n3 + n6, status=(b.piles.status() if b.has_piles else 0) |
+                (b.cloth.status() if b.has_cloth else 0), alg_bytes=alg3 + alg6,
+                launches=args.steps * batch_launches_per_frame(b), kernel="k3_frames (gs) + k6_substeps (whole frame)",
+                roofline_parts=rl,
+                launch={"cloth": b.cloth.launch_info() if b.has_cloth else None,
+                        "piles": b.piles.launch_info() if b.has_piles else None, "autotune": tune,
+                        "scenes_this_rank": len(b.scene_ids), "scenes_total": len(specs),
+                        "build_s": round(build_s, 1), "residual_max": float(np.nanmax(all_res)),
+                        "residual_median": float(np.nanmedian(all_res)),
+                        "scenes_with_residual": int(np.isfinite(all_res).sum()), "vs_solo": checks,
                         "cloth_particles": n3, "cloth_rows": rows3, "boxes": n6, "pairs": npairs,
-                        "manifold_points": pts})
+                        "manifold_points_per_substep": round(points_total / max(args.steps * S, 1), 1)})
 
 
 def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
     if workload == "batch":
-        return time_batch(args, device, flush_buf, clocks)
+        return time_batch(args, device, flush_buf, clocks, rank, world)
     if workload in SIX_DOF:
-        return time_engine6(args, workload, device, flush_buf, clocks)
+        return time_engine6(args, workload, device, world, flush_buf, clocks)
     import ctypes as C
 
     import numpy as np
@@ -267,6 +354,8 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+    T = s.tensors
+    n_rows_dev = torch.zeros(args.steps, dtype=torch.int32, device=device)
     # a frame: one xpbd3_step; with self collision it replays the captured
     # graph of contact rebuild + frame kernel
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -279,6 +368,7 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
             e0.record(stream)
             N.check(L.xpbd3_step(s._h, 1, sp), "xpbd3_step")
             e2.record(stream)
+            n_rows_dev[k:k + 1].copy_(T["n_rows"])  # this frame's live rows (outside the events)
         torch.cuda.synchronize(device)
     frame_ms = [a.elapsed_time(c) for a, c in ev]
     status = s.status()
@@ -286,7 +376,7 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
     types, counts = np.unique(rows["type"], return_counts=True)
     type_counts = {int(t): int(c) for t, c in zip(types, counts)}
     m = int(len(rows["type"]))
-    proj_per_frame = m * s.substeps * s.iterations
+    proj_total = int(n_rows_dev.sum().item()) * s.substeps * s.iterations
     total_ms = sum(frame_ms)
     kern_ms = frame_ms
     if s._self_collision:
@@ -305,19 +395,19 @@ def time_engine(args, workload, device, rank, world, flush_buf, clocks=None):
         torch.cuda.synchronize(device)
         kern_ms = [a.elapsed_time(c) for a, c in kev]
     alg_bytes = algorithmic_bytes(s, type_counts, gs)
-    res = dict(total_ms=total_ms, frame_ms=frame_ms, kern_ms=kern_ms, proj_per_frame=proj_per_frame,
+    launch = s.launch_info()
+    barriers, phases = s.phases()
+    res = dict(total_ms=total_ms, frame_ms=frame_ms, kern_ms=kern_ms, proj_total=proj_total,
                rows=m, bodies=s.num_bodies, status=status, alg_bytes=alg_bytes,
-               launches=launches_per_frame * args.steps, solver=s)
-    blocks, threads, smem = C.c_int(), C.c_int(), C.c_int()
-    L.xpbd3_launch_info(s._h, C.byref(blocks), C.byref(threads), C.byref(smem))
-    res["launch"] = dict(s.launch_info(), autotune=tune["ms_per_frame"])
+               launches=launches_per_frame * args.steps, solver=s, kernel="k3_frames",
+               latency=latency_model("k3_frames", statistics.mean(kern_ms), barriers, phases, launch, device))
+    res["launch"] = dict(launch, autotune=tune["ms_per_frame"])
     return res
 
 
-def time_engine6(args, workload, device, flush_buf, clocks=None):
+def time_engine6(args, workload, device, world, flush_buf, clocks=None):
     """Box pile: per frame the device broad phase (LBVH build + pair emission)
     then one persistent launch of all substeps."""
-    import numpy as np
     import torch
 
     from xpbd_b200 import Solver6DOF
@@ -334,10 +424,13 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
         N.check(L.xpbd6_step(s._h, 1, sp))
     tune = pin_or_tune(s, args)
     torch.cuda.synchronize(device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     ctx = clocks if clocks is not None else _Null()
-    pts = []
+    s.manifold_points(reset=True)
     with ctx:
         for k in range(args.steps):
             if flush_buf is not None:
@@ -351,12 +444,10 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
         torch.cuda.synchronize(device)
     frame_ms = [a.elapsed_time(c) for a, _, c in ev]
     kern_ms = [b.elapsed_time(c) for _, b, c in ev]
-    # rows of the last timed frame (before anything else advances the pile)
+    points_total = s.manifold_points()  # every substep of the timed frames
     n = s.num_bodies
     n_dyn = int((s.tensors["x"][:, 3] > 0).sum().item())
     npairs = min(s.n_pairs, s.cap)
-    hdr = s.tensors["m_hdr"][:npairs].cpu().numpy()
-    points = int(hdr[:, 0].sum())
     # graph replay of the whole frame (broad phase + substeps), back to back
     g0 = torch.cuda.Event(enable_timing=True)
     g1 = torch.cuda.Event(enable_timing=True)
@@ -366,23 +457,28 @@ def time_engine6(args, workload, device, flush_buf, clocks=None):
     torch.cuda.synchronize(device)
     graph_ms = g0.elapsed_time(g1) / args.steps
     status = s.status()
-    rows = 8 * n_dyn + points + s.num_joints
-    proj_per_frame = rows * s.substeps * s.iterations
     S, I = s.substeps, s.iterations
-    alg = S * (I * (points * 196 + 8 * n_dyn * 47 + s.num_joints * 196) + npairs * 300 + n * 128)
-    return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=kern_ms, proj_per_frame=proj_per_frame,
-                rows=rows, bodies=n, status=status, alg_bytes=alg, launches=args.steps * 2, solver=s,
-                kernel="k6_substeps8" if s.lanes == 8 else "k6_substeps",
-                launch=dict(s.launch_info(), pairs=npairs, manifold_points=points,
+    proj_total = I * (args.steps * S * (8 * n_dyn + s.num_joints) + points_total)
+    pts_sub = points_total / (args.steps * S)
+    alg = algorithmic_bytes6(S, I, n, n_dyn, s.num_joints, pts_sub, npairs)
+    kernel = "k6_substeps8" if s.lanes == 8 else "k6_substeps"
+    launch = s.launch_info()
+    barriers, phases = s.phases()
+    return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=kern_ms, proj_total=proj_total,
+                rows=int(round(8 * n_dyn + pts_sub + s.num_joints)), bodies=n, status=status, alg_bytes=alg,
+                launches=args.steps * 2, solver=s, kernel=kernel,
+                latency=latency_model(kernel, statistics.mean(kern_ms), barriers, phases, launch, device),
+                launch=dict(launch, pairs_last_frame=npairs, manifold_points_per_substep=round(pts_sub, 1),
                             graph_ms_per_frame=round(graph_ms, 5), autotune=tune["ms_per_frame"]))
 
 
 def time_e2e(args, workload, device):
     """Same metric through the public API with host buffers.  Every frame: the
     state (3-DOF: x, v; 6-DOF: x, q, v, w) is uploaded from pinned host memory,
-    ``step()`` runs, and the state is read back into pinned host memory, which
-    feeds the next frame; the stream is synchronised each frame.  The region is
-    bracketed by CUDA events on the solver's stream."""
+    ``step()`` runs, and the state (plus the live row count, 3-DOF) is read back
+    into pinned host memory, which feeds the next frame; the stream is
+    synchronised each frame.  The region is bracketed by CUDA events on the
+    solver's stream."""
     import torch
 
     from xpbd_b200 import Solver, Solver6DOF
@@ -396,35 +492,50 @@ def time_e2e(args, workload, device):
     T = s.tensors
     keys = ("x", "q", "v", "w") if six else ("x", "v")
     host = {k: T[k].cpu().pin_memory() for k in keys}
+    rows_host = torch.zeros(args.steps, dtype=torch.int32).pin_memory()
     stream = torch.cuda.current_stream(device)
 
-    def frame():
-        for k in keys:
-            T[k].copy_(host[k], non_blocking=True)
+    def frame(k=None):
+        for key in keys:
+            T[key].copy_(host[key], non_blocking=True)
         s.step()
-        for k in keys:
-            host[k].copy_(T[k], non_blocking=True)
+        for key in keys:
+            host[key].copy_(T[key], non_blocking=True)
+        if k is not None and not six:
+            rows_host[k:k + 1].copy_(T["n_rows"], non_blocking=True)
         stream.synchronize()
 
     for _ in range(SETTLE.get(workload, 0) + max(3, args.warmup)):  # the same frames as the device-timed leg
         frame()
     steps = args.steps
+    if six:
+        s.manifold_points(reset=True)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(steps):
-        frame()
+    for k in range(steps):
+        frame(k)
     e1.record(stream)
     torch.cuda.synchronize(device)
     ms = e0.elapsed_time(e1) / steps
+    S, I = s.substeps, s.iterations
     if six:
         n_dyn = int((T["x"][:, 3] > 0).sum().item())
-        hdr = T["m_hdr"][:min(s.n_pairs, s.cap)].cpu().numpy()
-        rows = 8 * n_dyn + int(hdr[:, 0].sum()) + s.num_joints
+        proj = I * (steps * S * (8 * n_dyn + s.num_joints) + s.manifold_points())
     else:
-        rows = s.num_constraints
+        proj = int(rows_host.sum().item()) * S * I
     nbytes = sum(host[k].numel() * 4 for k in keys)
-    return ms, rows * s.substeps * s.iterations, nbytes, nbytes
+    return ms, proj, nbytes, nbytes + (0 if six else 4)
+
+
+def frame_projections(s):
+    """Projections of the oracle's last frame: rows x S x I (3-DOF, the
+    reference's definition); I x (S x (8 floor slots per dynamic body + joints)
+    + the manifold points of every substep) (6-DOF)."""
+    if hasattr(s, "num_constraints"):
+        return s.num_constraints * s.substeps * s.iterations
+    n_dyn = int((s.inv_mass > 0).sum())
+    return s.iterations * (s.substeps * (8 * n_dyn + s.num_joints) + s.frame_points)
 
 
 def cpu_baseline(workload, seconds):
@@ -442,20 +553,11 @@ def cpu_baseline(workload, seconds):
     while True:
         s.step()
         frames += 1
-        proj += rows_of(s) * s.substeps * s.iterations
+        proj += frame_projections(s)
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
     return proj / dt / 1e6, frames, dt
-
-
-def rows_of(s):
-    """Projection rows of one substep: all rows (3-DOF, the reference's
-    definition); 8 floor slots per dynamic body + manifold points + joints (6-DOF)."""
-    if hasattr(s, "num_constraints"):
-        return s.num_constraints
-    n_dyn = int((s.inv_mass > 0).sum())
-    return 8 * n_dyn + int(s.m_count[:min(s.n_pairs, s.cap)].sum()) + s.num_joints
 
 
 class _Null:
@@ -488,6 +590,10 @@ def run_reference(args):
     t0 = time.perf_counter()
     from oracle import oracle as O
     six = args.workload in SIX_DOF
+    if args.workload == "batch":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched-scene path"}),
+              flush=True)
+        return
     s = make_solver(args.workload, "cpu", O.OracleSolver6DOF if six else O.OracleSolver)
     for _ in range(SETTLE.get(args.workload, 0) + args.warmup):
         s.step()
@@ -497,7 +603,7 @@ def run_reference(args):
         a = time.perf_counter()
         s.step()
         times.append(time.perf_counter() - a)
-        proj += rows_of(s) * s.substeps * s.iterations
+        proj += frame_projections(s)
     total = sum(times)
     value = proj / total / 1e6
     line = {
@@ -522,7 +628,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="spheres", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="boxes", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
@@ -552,13 +658,18 @@ def main():
     clocks = Clocks(local)
     r = time_engine(args, args.workload, device, rank, world, flush, clocks)
     total_ms = r["total_ms"]
+    proj_total = r["proj_total"]
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([total_ms], dtype=torch.float64, device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
+        pj = torch.tensor([proj_total], dtype=torch.float64, device=device)
+        dist.all_reduce(pj, op=dist.ReduceOp.SUM)
+        proj_total = float(pj.item())
     ms_per_step = total_ms / args.steps
-    value = world * r["proj_per_frame"] * args.steps / (total_ms / 1e3) / 1e6
+    value = proj_total / (total_ms / 1e3) / 1e6
+    sharded = args.workload == "batch"
     if rank == 0:
         hbm, peak_kind = peaks()
         kern_ms = statistics.mean(r["kern_ms"])
@@ -566,28 +677,36 @@ def main():
         line = {
             "metric": "constraint projections per second", "value": round(value, 4), "unit": "M proj/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "strong" if (sharded and world > 1) else "weak",
+            "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded numpy default_rng(0))",
-            "config": {"workload": WORKLOADS[args.workload], "bodies": r["bodies"], "rows_last_frame": r["rows"],
+            "config": {"workload": WORKLOADS[args.workload], "bodies": r["bodies"],
+                       "rows_per_substep": r["rows"], "projections_timed": int(proj_total),
                        "frames_per_step": 1, "settle_frames": SETTLE.get(args.workload, 0),
                        "l2": "flushed between frames (256 MB memset outside the timed events)",
-                       "parallelism": f"replicas x{world}", "launch": r["launch"]},
+                       "parallelism": (f"batch sharded over {world} ranks (LPT)" if sharded and world > 1
+                                       else f"replicas x{world}"), "launch": r["launch"]},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 5), "peak_kind": peak_kind,
-                         "traffic": traffic_for(args.workload),
-                         "kernel": r.get("kernel", {"batch": "k3_frames + k6_substeps (whole frame)"}.get(
-                             args.workload, "k3_frames")),
+                         "traffic": traffic_for(args.workload), "kernel": r["kernel"],
                          "kernel_ms": round(kern_ms, 5), "alg_bytes_per_launch": r["alg_bytes"]},
             "gpu_launches": r["launches"],
             "status_bits": r["status"],
         }
+        if "latency" in r:
+            line["latency"] = r["latency"]
+        if "roofline_parts" in r:
+            line["roofline"]["parts"] = r["roofline_parts"]
         line["clocks"] = clocks.summary()
         if args.kernels_only or args.workload == "batch":
             print(json.dumps(line), flush=True)
+            if world > 1:
+                import torch.distributed as dist
+                dist.destroy_process_group()
             return
         try:
             e_ms, e_proj, h2d, d2h = time_e2e(args, args.workload, device)
-            line["e2e"] = {"value": round(world * e_proj / (e_ms / 1e3) / 1e6, 4), "unit": "M proj/s",
+            line["e2e"] = {"value": round(world * e_proj / args.steps / (e_ms / 1e3) / 1e6, 4), "unit": "M proj/s",
                            "ms_per_step": round(e_ms, 5), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
         except Exception as e:  # pragma: no cover - reported, never silent
             line["e2e"] = {"error": repr(e)}
@@ -605,9 +724,19 @@ def main():
                     a2.steps = min(args.steps, 50)
                     rr = time_engine(a2, wl, device, 0, 1, flush, None)
                     ms = rr["total_ms"] / a2.steps
-                    extras[wl] = {"ms_per_frame": round(ms, 5),
-                                  "M_proj_per_s": round(rr["proj_per_frame"] / (ms / 1e3) / 1e6, 3),
-                                  "kernel_ms": round(statistics.mean(rr["kern_ms"]), 5), "launch": rr["launch"]}
+                    km = statistics.mean(rr["kern_ms"])
+                    ex = {"ms_per_frame": round(ms, 5),
+                          "M_proj_per_s": round(rr["proj_total"] / (rr["total_ms"] / 1e3) / 1e6, 3),
+                          "kernel_ms": round(km, 5), "launch": rr["launch"],
+                          "roofline": {"kernel": rr["kernel"], "alg_bytes_per_launch": rr["alg_bytes"],
+                                       "achieved_gbs": round(rr["alg_bytes"] / (km / 1e3) / 1e9, 2),
+                                       "frac": round(rr["alg_bytes"] / (km / 1e3) / 1e9 / hbm, 5),
+                                       "traffic": traffic_for(wl)}}
+                    if "latency" in rr:
+                        ex["latency"] = rr["latency"]
+                    if "roofline_parts" in rr:
+                        ex["roofline"]["parts"] = rr["roofline_parts"]
+                    extras[wl] = ex
                 line["other_workloads"] = extras
         print(json.dumps(line), flush=True)
     if world > 1:

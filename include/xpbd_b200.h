@@ -53,6 +53,14 @@ const char* xpbd_last_error(void);
  * word to *status_out (host memory) and synchronizes the stream; the context
  * stays usable. */
 int xpbd_barrier_selftest(int blocks, int absent, int rounds, int* status_out, void* stream);
+/* Latency floor of one frame-kernel phase (no reference counterpart; the
+ * denominator of the benchmark's latency fraction): `rounds` phases in which
+ * every thread makes one dependent L2 load and one vector reduction and then
+ * arrives at the barrier of driver `mode` (0 cooperative grid with the bounded
+ * ticket barrier, 1 one CTA, 2 one thread-block cluster of 2-16 CTAs), on
+ * `blocks` CTAs of `threads` threads.  Writes the mean ns per phase to
+ * *ns_per_phase (host memory); synchronizes the stream. */
+int xpbd_phase_floor(int mode, int blocks, int threads, int rounds, float* ns_per_phase, void* stream);
 
 /* ========================================================================== */
 /* 3-DOF particle solver (replaces solver.py:57-508 + kernels.py)              */
@@ -116,6 +124,9 @@ int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int* smem_byte
  * 1 one CTA with the particle state in shared memory, 2 one thread-block
  * cluster (2-16 CTAs, hardware cluster barrier); blocks/threads 0 = automatic. */
 int xpbd3_set_driver(xpbd3_solver* h, int mode, int blocks, int threads);
+/* Barriers and phases (work between barriers) of one frame of the bound frame
+ * kernel (no reference counterpart; the benchmark's latency model). */
+int xpbd3_phases(xpbd3_solver* h, int* barriers, int* phases);
 
 /* Constraint residual after a solve (no reference counterpart; the metric of
  * the benchmark and of the learned warm start): hard rows max(0, -C),
@@ -293,6 +304,15 @@ int xpbd6_set_lanes(xpbd6_solver* h, int lanes);
 int xpbd6_manifold8(const xpbd6_state* s, float margin, void* stream);
 /* blocks (negative = cluster of that many CTAs) and threads of the substep kernel. */
 int xpbd6_launch_info(xpbd6_solver* h, int* blocks, int* threads);
+/* Barriers and phases of one frame of the bound substep kernel (no reference
+ * counterpart; the benchmark's latency model). */
+int xpbd6_phases(xpbd6_solver* h, int* barriers, int* phases);
+/* Manifold points summed over every substep the handle's substep kernel has run
+ * since the last reset (no reference counterpart; the benchmark's projection
+ * count is I x (8 floor slots per dynamic body + points + joints) per substep).
+ * Copies the count to *total (host memory), clears it when reset != 0, and
+ * synchronizes the stream. */
+int xpbd6_points(xpbd6_solver* h, unsigned long long* total, int reset, void* stream);
 /* Host constants of the hash-grid / grid broad phases (solver_6dof.py:335-337,
  * 244): largest bounding radius |he|, hash-grid cell, largest |he| for the grid margin. */
 int xpbd6_set_grid_constants(xpbd6_solver* h, double rs_max, double cell, double max_he);

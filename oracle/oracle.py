@@ -61,6 +61,7 @@ def lib():
         L.or3_color_ranges.restype = C.c_int
         L.or3_residual.restype = C.c_float
         L.or6_residual.restype = C.c_float
+        L.or6_frame.restype = C.c_int64
     return _LIB
 
 
@@ -628,7 +629,8 @@ class OracleSolver6DOF:
         if len(self._x) == 0:
             return
         self.n_pairs = self._broadphase()
-        lib().or6_frame(C.byref(self._scene()), C.byref(self._params()))
+        # manifold points summed over this frame's substeps (the projection count)
+        self.frame_points = int(lib().or6_frame(C.byref(self._scene()), C.byref(self._params())))
 
     def residual(self):
         """Max residual of the last frame's joints, floor corners and manifold points."""

@@ -1023,15 +1023,18 @@ void or6_cap(const or6_scene *S, float max_lin, float max_ang) {
     }
 }
 
-/* solver_6dof.py:357-426 _record: one frame of substeps on a fixed pair list */
-void or6_frame(const or6_scene *S, const or6_params *P) {
+/* solver_6dof.py:357-426 _record: one frame of substeps on a fixed pair list.
+ * Returns the manifold points summed over the substeps (projection count). */
+int64_t or6_frame(const or6_scene *S, const or6_params *P) {
     float h = (float)(P->dt / (double)P->substeps);
+    int64_t points = 0;
     for (int s = 0; s < P->substeps; ++s) {
         or6_integrate(S, P->gx, P->gy, P->gz, h, P->gyroscopic);
         memset(S->lam_floor, 0, sizeof(float) * 8 * (size_t)S->n);
         memset(S->lam_pair, 0, sizeof(float) * 8 * (size_t)S->cap);
         if (S->n_joints) memset(S->lam_joint, 0, sizeof(float) * (size_t)S->n_joints);
         or6_manifold(S, P->man_margin);
+        for (int p = 0; p < S->n_pairs; ++p) points += S->m_count[p];
         for (int it = 0; it < P->iterations; ++it) {
             if (S->n_joints) or6_solve_joints(S, h);
             or6_solve_floor(S, P->floor_y, P->friction);
@@ -1044,6 +1047,7 @@ void or6_frame(const or6_scene *S, const or6_params *P) {
         or6_apply_velocity(S);
         if (P->max_speed > 0.0f) or6_cap(S, P->max_speed, P->max_omega);
     }
+    return points;
 }
 
 /* ---------------------------------------------------------------------- */

@@ -65,3 +65,32 @@ def test_batch_specs_distribution():
     pi = [s.size for s in sp if s.kind == "pile"]
     assert len(cl) == len(pi) == 128
     assert min(cl) >= 16 and max(cl) <= 128 and min(pi) >= 64 and max(pi) <= 1024
+
+
+def test_sharded_batch_holds_only_its_scenes():
+    """A rank's share of a sharded batch (scene_ids): only those scenes are
+    built, each still evolves exactly as when solved alone, and the residuals of
+    the scenes held elsewhere are NaN (the all-gather fills them in)."""
+    specs = _small_specs()
+    mine = [1, 2, 4, 6]
+    b = BatchedScenes(specs, substeps=10, iterations=2, scene_ids=mine)
+    assert b.scene_ids == mine
+    assert sorted(b.cloth_ids + b.pile_ids) == mine
+    assert b.cloth.num_bodies == sum(specs[i].size ** 2 for i in mine if specs[i].kind == "cloth")
+    assert b.piles.num_bodies == sum(specs[i].size for i in mine if specs[i].kind == "pile")
+    solos = {i: b.solo(i) for i in mine}
+    b.reset_projection_count()
+    for _ in range(4):
+        b.step()
+        for s in solos.values():
+            s.step()
+    torch.cuda.synchronize()
+    res = b.residuals()
+    for i in range(len(specs)):
+        if i not in mine:
+            assert np.isnan(res[i])
+            continue
+        d = np.abs(b.scene_positions(i) - solos[i].positions()).max()
+        assert d <= (0.0 if specs[i].kind == "cloth" else 1e-4), (i, d)
+    # projections: cloth rows x S x I per frame plus the pile substeps' counted points
+    assert b.projections(4) > 4 * 10 * 2 * b.cloth.num_constraints

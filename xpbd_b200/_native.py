@@ -85,6 +85,9 @@ _SIGS = {
     "xpbd3_contacts_build": ([_p, _p, _p, _p, _p, C.c_int, _p, C.c_int, _p, C.c_double, C.c_double,
                               C.c_double, _p, _p], C.c_int),
     "xpbd_barrier_selftest": ([C.c_int, C.c_int, C.c_int, _p, _p], C.c_int),
+    "xpbd_phase_floor": ([C.c_int, C.c_int, C.c_int, C.c_int, _p, _p], C.c_int),
+    "xpbd3_phases": ([_p, _ip, _ip], C.c_int),
+    "xpbd6_phases": ([_p, _ip, _ip], C.c_int),
     "xpbd3_attach_contacts": ([_p, _p, _p, _p, _p, C.c_int, _p, C.c_int, _p, C.c_double, C.c_double,
                                C.c_double, _p], C.c_int),
     "xpbd_sort_pairs_u64": ([_p, _p, C.c_int, C.c_int, _p], C.c_int),

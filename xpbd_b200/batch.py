@@ -75,9 +75,59 @@ CLOTH_KW = dict(dt=1 / 60, substeps=15, iterations=2)
 PILE_KW = dict(dt=1 / 60, substeps=15, iterations=2, floor_y=0.0, friction=0.6, restitution=0.2, broadphase="lbvh")
 
 
+@dataclass
+class BatchLayout:
+    """Where each scene of a (possibly partial) batch sits in the two packed
+    systems: global scene ids, body ranges and cloth row ranges."""
+    cloth_ids: list
+    pile_ids: list
+    cloth_bodies: list   # (b0, b1) per cloth scene, in the 3-DOF system
+    cloth_rows: list     # (r0, r1) per cloth scene
+    pile_bodies: list    # (b0, b1) per pile scene, in the 6-DOF system
+
+
+def build_batch(specs, scene_ids, cloth, piles) -> BatchLayout:
+    """Add the scenes `scene_ids` (global indices into `specs`, ascending) to a
+    3-DOF solver `cloth` and a 6-DOF solver `piles` through the public
+    scene-building API.  Each pile is opened as its own scene when the solver
+    supports scene ids (``begin_scene``), so no pair ever joins two scenes."""
+    lay = BatchLayout([], [], [], [], [])
+    pile_scene = 0
+    for i in scene_ids:
+        sp = specs[i]
+        if sp.kind == "cloth":
+            b0, r0 = cloth.num_bodies, cloth.num_constraints
+            build_cloth_scene(cloth, sp.size)
+            lay.cloth_ids.append(i)
+            lay.cloth_bodies.append((b0, cloth.num_bodies))
+            lay.cloth_rows.append((r0, cloth.num_constraints))
+        else:
+            b0 = piles.num_bodies
+            if hasattr(piles, "begin_scene"):
+                piles.begin_scene(pile_scene)
+            build_pile_k(piles, sp.size, sp.seed)
+            lay.pile_ids.append(i)
+            lay.pile_bodies.append((b0, piles.num_bodies))
+            pile_scene += 1
+    return lay
+
+
+def rank_scene_ids(specs, rank: int, world: int):
+    """The scenes one rank of `world` steps: LPT bin packing of the scenes'
+    projection counts (``shard.lpt_partition``), so every scene is stepped by
+    exactly one rank and the ranks' loads are balanced."""
+    from .shard import lpt_partition, scene_cost
+    if world <= 1:
+        return list(range(len(specs)))
+    return lpt_partition([scene_cost(sp) for sp in specs], world)[rank]
+
+
 class BatchedScenes:
-    def __init__(self, specs, device="cuda:0", cloth_mode="gs", substeps=15, iterations=2):
+    def __init__(self, specs, device="cuda:0", cloth_mode="gs", substeps=15, iterations=2, scene_ids=None):
+        """`scene_ids`: the global indices of the scenes this instance steps (a
+        rank's share of a sharded batch, see ``rank_scene_ids``); None = all."""
         self.specs = list(specs)
+        self.scene_ids = list(range(len(self.specs))) if scene_ids is None else sorted(int(i) for i in scene_ids)
         self.device = device
         self.cloth_mode = cloth_mode
         kw3 = dict(CLOTH_KW, substeps=substeps, iterations=iterations)
@@ -85,25 +135,11 @@ class BatchedScenes:
         self.cloth = Solver(device=device, solve_mode=cloth_mode, **kw3)
         self.piles = Solver6DOF(device=device, **kw6)
         self.piles.sync_pairs = False
-        self.cloth_ids, self.pile_ids = [], []
-        self.cloth_rows, self.cloth_bodies, self.pile_bodies = [], [], []
-        groups = []
-        pile_scene = 0
-        for i, sp in enumerate(self.specs):
-            if sp.kind == "cloth":
-                b0, r0 = self.cloth.num_bodies, len(self.cloth._rows)
-                build_cloth_scene(self.cloth, sp.size)
-                self.cloth_ids.append(i)
-                self.cloth_bodies.append((b0, self.cloth.num_bodies))
-                self.cloth_rows.append((r0, len(self.cloth._rows)))
-                groups.append((r0, len(self.cloth._rows)))
-            else:
-                b0 = self.piles.num_bodies
-                self.piles.begin_scene(pile_scene)
-                build_pile_k(self.piles, sp.size, sp.seed)
-                self.pile_ids.append(i)
-                self.pile_bodies.append((b0, self.piles.num_bodies))
-                pile_scene += 1
+        lay = build_batch(self.specs, self.scene_ids, self.cloth, self.piles)
+        self.layout = lay
+        self.cloth_ids, self.pile_ids = lay.cloth_ids, lay.pile_ids
+        self.cloth_rows, self.cloth_bodies, self.pile_bodies = lay.cloth_rows, lay.cloth_bodies, lay.pile_bodies
+        groups = list(lay.cloth_rows)
         self.cloth.color_groups = groups
         self.has_cloth = self.cloth.num_bodies > 0
         self.has_piles = self.piles.num_bodies > 0
@@ -142,6 +178,8 @@ class BatchedScenes:
         cur.wait_stream(self.stream_piles)
 
     def projections_per_frame(self):
+        """Projections of one frame with the manifold points of the last substep
+        (an estimate; ``projections`` counts every substep)."""
         S, I = self.cloth.substeps, self.cloth.iterations
         n3 = self.cloth.num_constraints if self.has_cloth else 0
         if not self.has_piles:
@@ -152,9 +190,27 @@ class BatchedScenes:
         n6 = 8 * n_dyn + int(hdr[:, 0].sum()) + self.piles.num_joints
         return (n3 + n6) * S * I
 
+    def reset_projection_count(self):
+        if self.has_piles:
+            self.piles.manifold_points(reset=True)
+
+    def projections(self, frames):
+        """Projections of the last `frames` frames since ``reset_projection_count``:
+        cloth rows x S x I per frame, and per pile substep I x (8 floor slots per
+        dynamic body + that substep's manifold points + joints), the points
+        counted on the device (synchronizes)."""
+        S, I = self.cloth.substeps, self.cloth.iterations
+        total = frames * S * I * (self.cloth.num_constraints if self.has_cloth else 0)
+        if self.has_piles:
+            T = self.piles.tensors
+            n_dyn = int((T["x"][:, 3] > 0).sum().item())
+            total += I * (frames * S * (8 * n_dyn + self.piles.num_joints) + self.piles.manifold_points())
+        return total
+
     def residuals(self):
-        """Max residual per scene, indexed like `specs`."""
-        out = np.zeros(len(self.specs), np.float32)
+        """Max residual per scene, indexed like `specs` (NaN for scenes this
+        instance does not hold)."""
+        out = np.full(len(self.specs), np.nan, np.float32)
         rc = self.cloth.residual(self.row_scene, len(self.cloth_ids)) if self.has_cloth else []
         rp = self.piles.residual(self.body_scene, max(len(self.pile_ids), 1)) if self.has_piles else []
         for k, i in enumerate(self.cloth_ids):

@@ -112,7 +112,85 @@ __global__ void k_barrier_selftest(GridBarrier b, int absent, int rounds) {
   grid_exit(b);
 }
 
+// Phase floor probe: `rounds` phases of the least dependent work a frame
+// kernel's phase contains.  Every thread loads one float4 that another CTA
+// reduced into in the previous phase (an L2 round trip, ld.global.cg), adds it
+// into another slot with one vector reduction (which the barrier's release then
+// waits for), and arrives at the barrier of the driver being modelled (the
+// grid ticket barrier, the hardware cluster barrier, or __syncthreads for one
+// CTA).  Thread 0 of CTA 0 times the rounds with the global timer.
+__global__ void k_phase_floor(GridBarrier b, float4* buf, int rounds, unsigned long long* ns_out) {
+  const int t = gtid(), T = gstride();
+  grid_sync(b);
+  const uint64_t t0 = global_ns();
+  for (int r = 0; r < rounds; ++r) {
+    const int src = (t + (r + 1) * (int)blockDim.x) % T;
+    const float4 v = __ldcg(buf + (size_t)(r & 1) * T + src);
+    red_add4(buf + (size_t)((r + 1) & 1) * T + (t + (int)blockDim.x) % T, v);
+    grid_sync(b);
+  }
+  const uint64_t t1 = global_ns();
+  if (t == 0) *ns_out = t1 - t0;
+  grid_exit(b);
+}
+
 }  // namespace xpbd
+
+extern "C" int xpbd_phase_floor(int mode, int blocks, int threads, int rounds, float* ns_per_phase, void* stream) {
+  using namespace xpbd;
+  if (!ns_per_phase || rounds < 1 || rounds > 100000 || threads < 32 || threads > 1024 || threads % 32 ||
+      blocks < 1 || (mode != 0 && mode != 1 && mode != 2) || (mode == 1 && blocks != 1) ||
+      (mode == 2 && (blocks < 2 || blocks > 16)))
+    return XPBD_ERR_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  if (mode == 2) {
+    XPBD_CUDA(cudaFuncSetAttribute(k_phase_floor, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = blocks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    XPBD_CUDA(cudaOccupancyMaxActiveClusters(&nc, k_phase_floor, &cfg));
+    if (nc < 1) return XPBD_ERR_BAD_ARG;
+  } else if (mode == 0) {
+    int per_sm = 0;
+    XPBD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase_floor, threads, 0));
+    if (blocks > per_sm * num_sms()) return XPBD_ERR_BAD_ARG;  // a cooperative grid must be co-resident
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = blocks > 1 ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  const size_t T = (size_t)blocks * threads;
+  unsigned char* mem = nullptr;
+  XPBD_CUDA(cudaMalloc(&mem, 256 + 2 * T * sizeof(float4)));
+  unsigned* bar = reinterpret_cast<unsigned*>(mem);
+  unsigned long long* ns = reinterpret_cast<unsigned long long*>(mem + 64);
+  float4* buf = reinterpret_cast<float4*>(mem + 256);
+  unsigned long long ns_host = 0;
+  cudaError_t e = cudaMemsetAsync(mem, 0, 256 + 2 * T * sizeof(float4), st);
+  GridBarrier gb = make_grid_barrier(bar, mode == 2 ? 1 : 0);
+  if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, k_phase_floor, gb, buf, rounds, ns);
+  int status = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ns_host, ns, sizeof(ns_host), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&status, bar + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(mem);
+  if (e != cudaSuccess) {
+    set_last_error("xpbd_phase_floor", e);
+    return XPBD_ERR_CUDA;
+  }
+  if (status & XPBD_ERR_BARRIER_TIMEOUT) return XPBD_ERR_CUDA;
+  *ns_per_phase = (float)((double)ns_host / rounds);
+  return XPBD_OK;
+}
 
 extern "C" int xpbd_barrier_selftest(int blocks, int absent, int rounds, int* status_out, void* stream) {
   using namespace xpbd;

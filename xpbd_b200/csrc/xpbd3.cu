@@ -1271,6 +1271,36 @@ extern "C" int xpbd3_status(xpbd3_solver* h, int* out, void* stream) {
   return XPBD_OK;
 }
 
+// Barriers and phases of one frame of k3_frames as bound (the same conditions
+// the kernel tests; the live row count is taken as nonzero when rows exist).
+// A phase is the work between two barriers; the folded-boundary path ends with
+// a closing pass after its last barrier.
+extern "C" int xpbd3_phases(xpbd3_solver* h, int* barriers, int* phases) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  const Par3& q = h->p3;
+  const bool rows = h->st.row_capacity > 0 && h->st.n_bodies > 0;
+  const int S = q.substeps, I = q.iterations;
+  const bool smem = h->mode == 1;
+  long long b = 0, ph = 0;
+  if (!q.gs && !smem && q.fold && q.carry && rows) {
+    b = (long long)S * I;
+    ph = b + 1;
+  } else {
+    b = 1 + ((q.gs && !smem && q.gs_gpacked && rows) ? 1 : 0);
+    long long per_sub = 1;
+    if (rows) {
+      if (q.gs) per_sub += (long long)I * h->dev.ncolors;
+      else if (!smem && q.fold) per_sub += I;
+      else per_sub += I + (I > 0 ? I - 1 : 0);
+    }
+    b += (long long)S * per_sub;
+    ph = b;
+  }
+  if (barriers) *barriers = (int)b;
+  if (phases) *phases = (int)ph;
+  return XPBD_OK;
+}
+
 extern "C" int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int* smem_bytes) {
   if (!h) return XPBD_ERR_BAD_ARG;
   if (blocks) *blocks = h->mode == 2 ? -h->blocks : h->blocks;

@@ -38,8 +38,18 @@ struct Dev6 {
   const float4* j_b;  // anchor in B's frame, compliance in w
   float* lam_joint;
   const int* scene;  // per body (NULL: one scene)
+  // manifold points summed over the substeps of every frame run (NULL: not
+  // counted); the benchmark's projection count
+  unsigned long long* points;
   int n, nj, cap, n_scenes;
 };
+
+// Adds each thread's count of manifold points to *points, one atomic per warp.
+XD void add_points(unsigned long long* points, unsigned pts) {
+  if (!points) return;
+  for (int o = 16; o > 0; o >>= 1) pts += __shfl_xor_sync(0xffffffffu, pts, o);
+  if ((threadIdx.x & 31) == 0 && pts) atomicAdd(points, (unsigned long long)pts);
+}
 
 struct Par6 {
   float h, dt, gx, gy, gz, floor_y, mu, rest, lin_damp, ang_damp, relax, max_speed, max_omega, margin;
@@ -306,10 +316,10 @@ XD void manifold_pair(const Dev6& s, int pid, float margin, int edge_axes = 0) {
 }
 
 // ---- kernels_6dof.py:386-430 solve_box_manifold, one pair -------------------------
-XD void box_pair(const Dev6& s, int pid) {
+XD int box_pair(const Dev6& s, int pid) {  // returns the pair's manifold point count
   int4 hdr = s.m_hdr[pid];
   const int nc = hdr.x;
-  if (nc == 0) return;
+  if (nc == 0) return 0;
   const int inc = hdr.y, ref = hdr.z;
   V3 S = v3(s.m_normal[pid]);
   float4 xi4 = s.x[inc], xr4 = s.x[ref];
@@ -356,6 +366,7 @@ XD void box_pair(const Dev6& s, int pid) {
     vadd(s.ax + ref, dxr, cr);
     vadd(s.ar + ref, drr, 0.0f);
   }
+  return nc;
 }
 
 // ---- kernels_6dof.py:441-483 solve_joints, one joint --------------------------------
@@ -764,7 +775,7 @@ XD void floor_body8(const Dev6& s, int i, const Par6& p, const Grp& G) {
   }
 }
 
-XD void box_pair8(const Dev6& s, int pid, const Grp& G) {
+XD int box_pair8(const Dev6& s, int pid, const Grp& G) {  // returns the pair's manifold point count
   // the pair's own records with the header (one round trip), the bodies next
   const int c = G.l;
   const int slot = 8 * pid + c;
@@ -772,7 +783,7 @@ XD void box_pair8(const Dev6& s, int pid, const Grp& G) {
   const float4 nrm = s.m_normal[pid], off_inc = s.m_off_inc[slot], off_ref = s.m_off_ref[slot];
   const float lam_slot = s.lam_pair[slot];
   const int nc = hdr.x;
-  if (nc == 0) return;
+  if (nc == 0) return 0;
   const int inc = hdr.y, ref = hdr.z;
   V3 S = v3(nrm);
   float4 xi4 = s.x[inc], xr4 = s.x[ref];
@@ -827,6 +838,7 @@ XD void box_pair8(const Dev6& s, int pid, const Grp& G) {
       vadd(s.ar + ref, drr, 0.0f);
     }
   }
+  return nc;
 }
 
 XD void velocity_floor8(const Dev6& s, int i, const Par6& p, const Grp& G) {
@@ -1069,6 +1081,7 @@ XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float
 __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier bar) {
   const int n = s.n, nj = s.nj;
   const int np = min(*s.n_pairs, s.cap);
+  unsigned pts = 0;  // manifold points of this thread's pairs, every substep
   const int t0 = gtid(), st = gstride();
   const int nb = max(n, nj);
   for (int i = t0; i < nb; i += st) {
@@ -1085,7 +1098,10 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
       for (int t = t0; t < work; t += st) {
         if (t < nj) joint_row(s, t, p.h);
         else if (t < nj + n) floor_body(s, t - nj, p);
-        else box_pair(s, t - nj - n);
+        else {
+          const int nc = box_pair(s, t - nj - n);
+          if (it == 0) pts += nc;
+        }
       }
       grid_sync(bar);
       const bool last = it + 1 == p.iterations;
@@ -1107,6 +1123,7 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
     }
     grid_sync(bar);
   }
+  add_points(s.points, pts);
   grid_exit(bar);
 }
 
@@ -1116,6 +1133,7 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
   __shared__ float4 stage[512 / 8][8];
   const int n = s.n, nj = s.nj;
   const int np = min(*s.n_pairs, s.cap);
+  unsigned pts = 0;  // manifold points of this thread's pairs, every substep
   const int t0 = gtid(), st = gstride();
   const Grp G = grp8();
   const int g0 = t0 >> 3, gs = st >> 3;
@@ -1134,7 +1152,10 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
       for (int t = t0; t < nj; t += st) joint_row(s, t, p.h);
       for (int g = g0; g < n + np; g += gs) {
         if (g < n) floor_body8(s, g, p, G);
-        else box_pair8(s, g - n, G);
+        else {
+          const int nc = box_pair8(s, g - n, G);
+          if (it == 0 && G.l == 0) pts += nc;
+        }
       }
       grid_sync(bar);
       const bool last = it + 1 == p.iterations;
@@ -1156,6 +1177,7 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
     }
     grid_sync(bar);
   }
+  add_points(s.points, pts);
   grid_exit(bar);
 }
 
@@ -2211,6 +2233,7 @@ static Dev6 make_dev6(const xpbd6_state* s) {
   d.j_b = reinterpret_cast<const float4*>(s->j_anchor_b);
   d.lam_joint = s->lam_joint;
   d.scene = s->scene;
+  d.points = nullptr;
   d.n_scenes = s->scene ? std::max(s->n_scenes, 1) : 1;
   d.n = s->n_bodies;
   d.nj = s->n_joints;
@@ -2337,14 +2360,25 @@ static void free_graph(xpbd6_solver* h) {
 extern "C" int xpbd6_create(xpbd6_solver** out) {
   if (!out) return XPBD_ERR_BAD_ARG;
   xpbd6_solver* h = new xpbd6_solver();
-  cudaError_t e = cudaMalloc(&h->bar, 4 * sizeof(unsigned));
+  // words 0-3: the grid barrier (count, status, exits); 4-5: the manifold point counter
+  cudaError_t e = cudaMalloc(&h->bar, 8 * sizeof(unsigned));
   if (e != cudaSuccess) {
     set_last_error("cudaMalloc", e);
     delete h;
     return XPBD_ERR_CUDA;
   }
-  cudaMemset(h->bar, 0, 4 * sizeof(unsigned));
+  cudaMemset(h->bar, 0, 8 * sizeof(unsigned));
   *out = h;
+  return XPBD_OK;
+}
+
+extern "C" int xpbd6_points(xpbd6_solver* h, unsigned long long* total, int reset, void* stream) {
+  if (!h || !total) return XPBD_ERR_BAD_ARG;
+  cudaStream_t st = as_stream(stream);
+  unsigned long long* ctr = reinterpret_cast<unsigned long long*>(h->bar + 4);
+  XPBD_CUDA(cudaMemcpyAsync(total, ctr, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  if (reset) XPBD_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), st));
+  XPBD_CUDA(cudaStreamSynchronize(st));
   return XPBD_OK;
 }
 
@@ -2426,6 +2460,7 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
   h->st = *s;
   h->par = *p;
   h->dev = make_dev6(s);
+  h->dev.points = reinterpret_cast<unsigned long long*>(h->bar + 4);
   h->p6 = make_par6(p);
   const int n = std::max(s->n_bodies, 2);
   size_t off = 0;
@@ -2690,6 +2725,19 @@ extern "C" int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream) 
   XPBD_CUDA(cudaMemcpyAsync(k.data(), h->bp.keys, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
   XPBD_CUDA(cudaStreamSynchronize(st));
   for (int i = 0; i < n; ++i) codes_out[i] = (unsigned)k[i];
+  return XPBD_OK;
+}
+
+// Barriers and phases of one frame of k6_substeps / k6_substeps8 as bound: the
+// integrate pass, then per substep the manifold, (solve, apply) per iteration
+// (a finalize pass when there are none), the velocity solve and the velocity
+// apply + integrate, each closed by a barrier.
+extern "C" int xpbd6_phases(xpbd6_solver* h, int* barriers, int* phases) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  const int S = h->par.substeps, I = h->par.iterations;
+  const long long b = 1 + (long long)S * (1 + (I > 0 ? 2 * I : 1) + 2);
+  if (barriers) *barriers = (int)b;
+  if (phases) *phases = (int)b;
   return XPBD_OK;
 }
 

@@ -323,6 +323,13 @@ class Solver:
         mode = "cluster" if b.value < 0 else ("shared" if sm.value > 0 else "grid")
         return {"mode": mode, "blocks": abs(b.value), "threads": t.value, "smem_bytes": sm.value}
 
+    def phases(self) -> tuple:
+        """(barriers, phases) of one frame of the bound frame kernel."""
+        self._flush()
+        b, ph = C.c_int(), C.c_int()
+        N.check(N.lib().xpbd3_phases(self._h, C.byref(b), C.byref(ph)), "xpbd3_phases")
+        return b.value, ph.value
+
     def autotune(self, frames: int = 3, candidates=None) -> dict:
         """Time the frame drivers on the current scene and keep the fastest."""
         from .autotune import tune3

@@ -83,6 +83,8 @@ _SIGS6 = {
     "xpbd6_apply_velocity": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "xpbd6_body_aabb": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "xpbd6_residual": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "xpbd6_phases": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "xpbd6_points": ([C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int, C.c_void_p], C.c_int),
 }
 
 
@@ -346,6 +348,24 @@ class Solver6DOF:
         b, t = C.c_int(), C.c_int()
         lib6().xpbd6_launch_info(self._h, C.byref(b), C.byref(t))
         return {"mode": "cluster" if b.value < 0 else "grid", "blocks": abs(b.value), "threads": t.value}
+
+    def phases(self):
+        """(barriers, phases) of one frame of the bound substep kernel."""
+        self._flush()
+        if self._sig != self._signature():
+            self._bind()
+        b, ph = C.c_int(), C.c_int()
+        N.check(lib6().xpbd6_phases(self._h, C.byref(b), C.byref(ph)), "xpbd6_phases")
+        return b.value, ph.value
+
+    def manifold_points(self, reset=False):
+        """Manifold points summed over every substep run since the last reset
+        (synchronizes the stream)."""
+        self._flush()
+        out = C.c_ulonglong(0)
+        N.check(lib6().xpbd6_points(self._h, C.byref(out), 1 if reset else 0, N.stream_of(self.device)),
+                "xpbd6_points")
+        return int(out.value)
 
     def autotune(self, frames=3, candidates=None):
         """Time the substep drivers on the current scene and keep the fastest."""
