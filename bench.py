@@ -538,13 +538,16 @@ def frame_projections(s):
     return s.iterations * (s.substeps * (8 * n_dyn + s.num_joints) + s.frame_points)
 
 
-def cpu_baseline(workload, seconds):
+def cpu_baseline(workload, seconds, threads=1):
     """The oracle (CPU restatement of the reference) on a bounded sample of the
     same workload: consecutive frames from the same initial state until
-    `seconds` of host time have elapsed (at least one frame)."""
+    `seconds` of host time have elapsed (at least one frame), its substep loop
+    on `threads` host threads (OpenMP; the contact rebuild and row flush stay
+    on the Python thread, as in the reference's own host code)."""
     from oracle import oracle as O
     six = workload in SIX_DOF
     s = make_solver(workload, "cpu", O.OracleSolver6DOF if six else O.OracleSolver)
+    s.threads = threads
     for _ in range(1 + SETTLE.get(workload, 0)):  # outside the sample: array set-up + the settling frames
         s.step()
     t0 = time.perf_counter()
@@ -595,6 +598,8 @@ def run_reference(args):
               flush=True)
         return
     s = make_solver(args.workload, "cpu", O.OracleSolver6DOF if six else O.OracleSolver)
+    threads = O.host_threads()  # every host core (OMP_NUM_THREADS when set)
+    s.threads = threads
     for _ in range(SETTLE.get(args.workload, 0) + args.warmup):
         s.step()
     times = []
@@ -613,9 +618,10 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": {"workload": WORKLOADS[args.workload], "frames_per_step": 1,
                    "settle_frames": SETTLE.get(args.workload, 0)},
-        "cpu_baseline": {"value": round(value, 4), "unit": "M proj/s", "cores": 1, "kind": "port",
+        "cpu_baseline": {"value": round(value, 4), "unit": "M proj/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} consecutive frames after "
-                                   f"{SETTLE.get(args.workload, 0) + args.warmup} untimed frames"},
+                                   f"{SETTLE.get(args.workload, 0) + args.warmup} untimed frames, substep loop "
+                                   f"on {threads} OpenMP threads"},
         "e2e": {"value": round(value, 4), "unit": "M proj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(time.perf_counter() - t0, 2),
     }
@@ -711,10 +717,16 @@ def main():
         except Exception as e:  # pragma: no cover - reported, never silent
             line["e2e"] = {"error": repr(e)}
         if world == 1:
-            v, frames, secs = cpu_baseline(args.workload, args.cpu_seconds)
-            line["cpu_baseline"] = {"value": round(v, 4), "unit": "M proj/s", "cores": 1, "kind": "port",
+            from oracle import oracle as O
+            threads = O.host_threads()
+            v, frames, secs = cpu_baseline(args.workload, args.cpu_seconds, threads)
+            v1, frames1, secs1 = cpu_baseline(args.workload, args.cpu_seconds / 2, 1)
+            line["cpu_baseline"] = {"value": round(v, 4), "unit": "M proj/s", "cores": threads, "kind": "port",
                                     "sample": f"{frames} consecutive frames of the same workload after "
-                                              f"{SETTLE.get(args.workload, 0)} settling frames ({secs:.1f} s)"}
+                                              f"{SETTLE.get(args.workload, 0)} settling frames ({secs:.1f} s), "
+                                              f"substep loop on {threads} OpenMP threads",
+                                    "single_thread": {"value": round(v1, 4), "cores": 1,
+                                                      "sample": f"{frames1} frames ({secs1:.1f} s)"}}
             if not args.no_extras:
                 extras = {}
                 for wl in WORKLOADS:

@@ -36,7 +36,7 @@ def build(force=False):
     src = os.path.join(HERE, "xpbd_oracle.c")
     if not force and os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= os.path.getmtime(src):
         return LIB_PATH
-    cmd = (f"gcc -O2 -ffp-contract=off -fno-fast-math -fPIC -shared -o {LIB_PATH}.tmp {src} -lm"
+    cmd = (f"gcc -O2 -ffp-contract=off -fno-fast-math -fopenmp -fPIC -shared -o {LIB_PATH}.tmp {src} -lm"
            f" && mv {LIB_PATH}.tmp {LIB_PATH}")
     if os.system(cmd) != 0:
         raise RuntimeError("failed to build the oracle library")
@@ -62,6 +62,9 @@ def lib():
         L.or3_residual.restype = C.c_float
         L.or6_residual.restype = C.c_float
         L.or6_frame.restype = C.c_int64
+        L.or6_frame_mt.restype = C.c_int64
+        L.or6_pairs_overlap_mt.restype = C.c_int64
+        L.or_max_threads.restype = C.c_int
     return _LIB
 
 
@@ -217,6 +220,10 @@ class OracleSolver:
         self.lam = None
         self.num_colors = 0
         self.color_counts = {}
+        # host threads of the substep loop: 1 = the sequential parity oracle;
+        # more = or3_frame_mt, the timed CPU baseline (Jacobi sums round in
+        # another order)
+        self.threads = 1
 
     # scene building (solver.py:130-228)
     def add_particle(self, position, mass, velocity=(0.0, 0.0, 0.0), shape=None, collide=True,
@@ -403,7 +410,10 @@ class OracleSolver:
         self._flush()
         if len(self._x) == 0:
             return
-        lib().or3_frame(C.byref(self._scene()), C.byref(self._params()))
+        if self.threads > 1:
+            lib().or3_frame_mt(C.byref(self._scene()), C.byref(self._params()), int(self.threads))
+        else:
+            lib().or3_frame(C.byref(self._scene()), C.byref(self._params()))
 
     def positions(self):
         return self.x.copy() if self.x is not None else _f32(self._x, (-1, 3))
@@ -476,6 +486,7 @@ class OracleSolver6DOF:
         self.x = self.q = self.v = self.omega = None
         self.n_pairs = 0
         self.cap = 0
+        self.threads = 1  # > 1: or6_frame_mt and the threaded pair emission (timed CPU baseline)
 
     def _add_body(self, position, half_extents, mass, quaternion, velocity, omega, color, static,
                   is_particle, group):
@@ -576,6 +587,10 @@ class OracleSolver6DOF:
         if self.broadphase == "lbvh":
             L.or6_body_aabb(n, fp(self.x), fp(self.q), fp(self.v), fp(self.omega), fp(self.he),
                             C.c_float(self._man_margin), C.c_float(self.dt), fp(self.lowers), fp(self.uppers))
+            if self.threads > 1:
+                return self._emit(lambda cap: L.or6_pairs_overlap_mt(
+                    n, fp(self.lowers), fp(self.uppers), fp(self.inv_mass), ip(self.group), C.c_int64(cap),
+                    ip(self.pair_a), ip(self.pair_b), int(self.threads)))
             return self._emit(lambda cap: L.or6_pairs_overlap(n, fp(self.lowers), fp(self.uppers),
                                                               fp(self.inv_mass), ip(self.group),
                                                               C.c_int64(cap), ip(self.pair_a), ip(self.pair_b)))
@@ -630,7 +645,11 @@ class OracleSolver6DOF:
             return
         self.n_pairs = self._broadphase()
         # manifold points summed over this frame's substeps (the projection count)
-        self.frame_points = int(lib().or6_frame(C.byref(self._scene()), C.byref(self._params())))
+        if self.threads > 1:
+            self.frame_points = int(lib().or6_frame_mt(C.byref(self._scene()), C.byref(self._params()),
+                                                       int(self.threads)))
+        else:
+            self.frame_points = int(lib().or6_frame(C.byref(self._scene()), C.byref(self._params())))
 
     def residual(self):
         """Max residual of the last frame's joints, floor corners and manifold points."""
@@ -660,6 +679,11 @@ class OracleSolver6DOF:
     @property
     def num_joints(self):
         return len(self._j_a)
+
+
+def host_threads():
+    """Threads the OpenMP runtime offers (OMP_NUM_THREADS, else the host's cores)."""
+    return int(lib().or_max_threads())
 
 
 def morton_codes(lowers, uppers):

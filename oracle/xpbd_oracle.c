@@ -1402,3 +1402,233 @@ void or_mlp_forward(const float *feats, int B, const float *w_in, float *y_out) 
         y_out[s] = y + x[3];
     }
 }
+
+/* ======================================================================== */
+/* Multi-threaded frames (OpenMP) -- the timed CPU baseline only.            */
+/*                                                                            */
+/* The same kernels as or3_frame / or6_frame, run on `nthreads` host threads: */
+/* per-body and per-pair passes on contiguous slices; Jacobi and velocity     */
+/* sums into per-thread accumulators, folded in thread order by the body's    */
+/* owner before it is applied; Gauss-Seidel rows of one color in parallel     */
+/* (rows of a color share no particle, so the color pass is bit-identical to  */
+/* the sequential one).  The Jacobi sums round differently from the          */
+/* sequential row order, so these frames are not the parity oracle: they are  */
+/* the reference's CPU path timed on every host core.                         */
+/* ======================================================================== */
+#include <omp.h>
+
+static inline void slice_range(int n, int t, int nt, int *a, int *b) {
+    *a = (int)((int64_t)n * t / nt);
+    *b = (int)((int64_t)n * (t + 1) / nt);
+}
+
+/* solver.py:412-467 substep loop, nthreads host threads */
+void or3_frame_mt(const or3_scene *S, const or3_params *P, int nthreads) {
+    int n = S->n_bodies, m = S->n_rows;
+    if (n == 0) return;
+    if (nthreads < 1) nthreads = 1;
+    float sdt = (float)(P->dt / (double)P->substeps);
+    float *pdx = (float *)calloc((size_t)nthreads * n * 3, sizeof(float));
+    int *pdn = (int *)calloc((size_t)nthreads * n, sizeof(int));
+#pragma omp parallel num_threads(nthreads)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        int i0, i1, j0, j1;
+        slice_range(n, t, nt, &i0, &i1);
+        slice_range(m, t, nt, &j0, &j1);
+        or3_scene R = *S; /* rows [j0, j1), this thread's accumulators */
+        R.n_rows = j1 - j0;
+        R.r_type += j0; R.r_a += j0; R.r_b += j0; R.r_active += j0;
+        R.r_rest += j0; R.r_comp += j0; R.r_anchor += 3 * j0; R.r_mu += j0; R.r_lambda += j0;
+        R.dx = pdx + (size_t)t * n * 3;
+        R.dn = pdn + (size_t)t * n;
+        for (int s = 0; s < P->substeps; ++s) {
+            or3_integrate(i1 - i0, S->x + 3 * i0, S->v + 3 * i0, S->inv_mass + i0, P->gx, P->gy, P->gz, sdt,
+                          S->x_prev + 3 * i0);
+            if (m > 0) {
+                memset(S->r_lambda + j0, 0, sizeof(float) * (size_t)(j1 - j0));
+#pragma omp barrier
+                for (int it = 0; it < P->iterations; ++it) {
+                    if (P->gs) {
+                        for (int c = 0; c < S->num_colors; ++c) {
+                            int start = S->color_starts[c];
+                            int count = S->color_starts[c + 1] - start;
+#pragma omp for schedule(static)
+                            for (int k = 0; k < count; ++k) or3_project_gs(S, S->color_order[start + k], sdt);
+                        }
+                    } else {
+                        or3_solve_jacobi_all(&R, sdt);
+#pragma omp barrier
+                        for (int i = i0; i < i1; ++i) {
+                            float ax = 0.0f, ay = 0.0f, az = 0.0f;
+                            int c = 0;
+                            for (int u = 0; u < nt; ++u) {
+                                float *d = pdx + ((size_t)u * n + i) * 3;
+                                ax += d[0]; ay += d[1]; az += d[2];
+                                c += pdn[(size_t)u * n + i];
+                                d[0] = d[1] = d[2] = 0.0f;
+                                pdn[(size_t)u * n + i] = 0;
+                            }
+                            if (c > 0 && S->inv_mass[i] > 0.0f)
+                                st3(S->x + 3 * i, add3(ld3(S->x + 3 * i), mul3(mk3(ax, ay, az),
+                                                                              P->jacobi_relax / (float)c)));
+                        }
+#pragma omp barrier
+                    }
+                }
+            } else {
+#pragma omp barrier
+            }
+            or3_finalize(i1 - i0, S->x + 3 * i0, S->x_prev + 3 * i0, S->inv_mass + i0, sdt, P->damping,
+                         S->v + 3 * i0);
+            if (P->max_speed > 0.0f && isfinite(P->max_speed)) or3_cap(i1 - i0, S->v + 3 * i0, P->max_speed);
+#pragma omp barrier
+        }
+    }
+    free(pdx);
+    free(pdn);
+}
+
+/* or6_pairs_overlap on nthreads host threads (same pairs, same order): each
+ * thread counts a contiguous range of i of about equal triangular work, the
+ * counts are scanned in thread order, then each thread writes its range. */
+int64_t or6_pairs_overlap_mt(int n, const float *lo, const float *hi, const float *inv_mass, const int *group,
+                             int64_t cap, int *pa, int *pb, int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    int64_t *cnt = (int64_t *)calloc((size_t)nthreads + 1, sizeof(int64_t));
+    int *bound = (int *)malloc(sizeof(int) * ((size_t)nthreads + 1));
+    /* boundaries: equal shares of sum_i (n - 1 - i) */
+    {
+        double total = 0.5 * (double)n * (double)(n - 1), acc = 0.0;
+        int t = 1;
+        bound[0] = 0;
+        for (int i = 0; i < n && t < nthreads; ++i) {
+            acc += (double)(n - 1 - i);
+            while (t < nthreads && acc >= total * t / nthreads) bound[t++] = i + 1;
+        }
+        while (t <= nthreads) bound[t++] = n;
+    }
+#pragma omp parallel num_threads(nthreads)
+    {
+        const int t = omp_get_thread_num();
+        for (int pass = 0; pass < 2; ++pass) {
+            int64_t c = 0, base = 0;
+            if (pass == 1) {
+                for (int u = 0; u < t; ++u) base += cnt[u];
+            }
+            for (int i = bound[t]; i < bound[t + 1]; ++i) {
+                for (int j = i + 1; j < n; ++j) {
+                    if (!(lo[3 * j] <= hi[3 * i] && lo[3 * j + 1] <= hi[3 * i + 1] &&
+                          lo[3 * j + 2] <= hi[3 * i + 2] && hi[3 * j] >= lo[3 * i] &&
+                          hi[3 * j + 1] >= lo[3 * i + 1] && hi[3 * j + 2] >= lo[3 * i + 2]))
+                        continue;
+                    if (inv_mass[i] == 0.0f && inv_mass[j] == 0.0f) continue;
+                    if (group[i] == group[j] && group[i] > 0) continue;
+                    if (pass == 1 && base + c < cap) { pa[base + c] = i; pb[base + c] = j; }
+                    ++c;
+                }
+            }
+            if (pass == 0) cnt[t] = c;
+#pragma omp barrier
+        }
+    }
+    int64_t total = 0;
+    for (int u = 0; u < nthreads; ++u) total += cnt[u];
+    free(cnt);
+    free(bound);
+    return total;
+}
+
+/* Body slice [i0, i1) of a 6-DOF scene (the passes that touch only body i). */
+static or6_scene or6_bodies(const or6_scene *S, int i0, int i1) {
+    or6_scene B = *S;
+    B.n = i1 - i0;
+    B.x += 3 * i0; B.q += 4 * i0; B.v += 3 * i0; B.w += 3 * i0; B.x_prev += 3 * i0; B.q_prev += 4 * i0;
+    B.inv_mass += i0; B.inv_I += 3 * i0; B.he += 3 * i0; B.group += i0;
+    B.dx += 3 * i0; B.drot += 3 * i0; B.dv += 3 * i0; B.dw += 3 * i0; B.dcount += i0; B.dvc += i0;
+    B.lam_floor += 8 * i0;
+    return B;
+}
+
+/* Folds the per-thread sums of body i into the shared ones (thread order). */
+static inline void fold6(float *dst3a, float *dst3b, int *dstc, const float *pa3, const float *pb3, const int *pc,
+                         int nt, int n, int i) {
+    v3 a = ld3(dst3a + 3 * i), b = ld3(dst3b + 3 * i);
+    int c = dstc[i];
+    for (int u = 0; u < nt; ++u) {
+        float *xa = (float *)pa3 + ((size_t)u * n + i) * 3, *xb = (float *)pb3 + ((size_t)u * n + i) * 3;
+        a = add3(a, ld3(xa));
+        b = add3(b, ld3(xb));
+        c += pc[(size_t)u * n + i];
+        xa[0] = xa[1] = xa[2] = 0.0f;
+        xb[0] = xb[1] = xb[2] = 0.0f;
+        ((int *)pc)[(size_t)u * n + i] = 0;
+    }
+    st3(dst3a + 3 * i, a);
+    st3(dst3b + 3 * i, b);
+    dstc[i] = c;
+}
+
+/* solver_6dof.py:357-426 on nthreads host threads; returns the manifold points
+ * summed over the substeps, like or6_frame. */
+int64_t or6_frame_mt(const or6_scene *S, const or6_params *P, int nthreads) {
+    const int n = S->n;
+    if (nthreads < 1) nthreads = 1;
+    float h = (float)(P->dt / (double)P->substeps);
+    const size_t pn = (size_t)nthreads * (size_t)(n > 0 ? n : 1);
+    float *px = (float *)calloc(pn * 3, sizeof(float)), *pr = (float *)calloc(pn * 3, sizeof(float));
+    float *pv = (float *)calloc(pn * 3, sizeof(float)), *pw = (float *)calloc(pn * 3, sizeof(float));
+    int *pc = (int *)calloc(pn, sizeof(int)), *pvc = (int *)calloc(pn, sizeof(int));
+    int64_t points = 0;
+#pragma omp parallel num_threads(nthreads) reduction(+ : points)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        int i0, i1, p0, p1, k0, k1;
+        slice_range(n, t, nt, &i0, &i1);
+        slice_range(S->cap, t, nt, &p0, &p1);
+        slice_range(S->n_joints, t, nt, &k0, &k1);
+        or6_scene B = or6_bodies(S, i0, i1);
+        or6_scene Q = *S; /* pairs [p0, p1) and joints [k0, k1); sums into this thread's accumulators */
+        Q.cap = p1 - p0;
+        Q.n_pairs = S->n_pairs - p0 < 0 ? 0 : (S->n_pairs - p0 > p1 - p0 ? p1 - p0 : S->n_pairs - p0);
+        Q.pair_a += p0; Q.pair_b += p0; Q.m_count += p0; Q.m_inc += p0; Q.m_ref += p0;
+        Q.m_normal += 3 * p0; Q.m_off_inc += 24 * p0; Q.m_off_ref += 24 * p0; Q.lam_pair += 8 * p0;
+        Q.n_joints = k1 - k0;
+        Q.j_a += k0; Q.j_b += k0; Q.j_anchor_a += 3 * k0; Q.j_anchor_b += 3 * k0; Q.j_rest += k0; Q.j_comp += k0;
+        Q.lam_joint += k0;
+        Q.dx = px + (size_t)t * n * 3; Q.drot = pr + (size_t)t * n * 3; Q.dcount = pc + (size_t)t * n;
+        Q.dv = pv + (size_t)t * n * 3; Q.dw = pw + (size_t)t * n * 3; Q.dvc = pvc + (size_t)t * n;
+        for (int s = 0; s < P->substeps; ++s) {
+            or6_integrate(&B, P->gx, P->gy, P->gz, h, P->gyroscopic);
+            memset(B.lam_floor, 0, sizeof(float) * 8 * (size_t)B.n);
+            memset(Q.lam_pair, 0, sizeof(float) * 8 * (size_t)Q.cap);
+            if (Q.n_joints) memset(Q.lam_joint, 0, sizeof(float) * (size_t)Q.n_joints);
+#pragma omp barrier
+            or6_manifold(&Q, P->man_margin);
+            for (int p = 0; p < Q.n_pairs; ++p) points += Q.m_count[p];
+#pragma omp barrier
+            for (int it = 0; it < P->iterations; ++it) {
+                if (Q.n_joints) or6_solve_joints(&Q, h);
+                or6_solve_floor(&B, P->floor_y, P->friction);
+                or6_solve_box(&Q);
+#pragma omp barrier
+                for (int i = i0; i < i1; ++i) fold6(S->dx, S->drot, S->dcount, px, pr, pc, nt, n, i);
+                or6_apply_jacobi(&B, P->jacobi_relax);
+#pragma omp barrier
+            }
+            or6_finalize(&B, h, P->lin_damp, P->ang_damp);
+#pragma omp barrier
+            or6_velocity_floor(&B, P->friction, P->restitution, h);
+            or6_velocity_box(&Q, P->friction, P->restitution, h);
+#pragma omp barrier
+            for (int i = i0; i < i1; ++i) fold6(S->dv, S->dw, S->dvc, pv, pw, pvc, nt, n, i);
+            or6_apply_velocity(&B);
+            if (P->max_speed > 0.0f) or6_cap(&B, P->max_speed, P->max_omega);
+#pragma omp barrier
+        }
+    }
+    free(px); free(pr); free(pv); free(pw); free(pc); free(pvc);
+    return points;
+}
+
+int or_max_threads(void) { return omp_get_max_threads(); }
