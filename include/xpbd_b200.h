@@ -141,6 +141,15 @@ int xpbd3_residual(const xpbd3_state* s, float h, const int* row_scene, int n_sc
 int xpbd_color_constraints(int n_bodies, int m, const int* a, const int* b, int* color);
 /* coloring.py:74-89 color_ranges (host). starts has num_colors+1 entries. */
 int xpbd_color_ranges(int m, const int* color, int* order, int* starts);
+/* coloring.py:26-89 on the device (the pass of a captured Gauss-Seidel frame
+ * with contacts): colors the live rows [0, *n_rows) of row_i (int4[row_capacity]:
+ * type, a, b (< 0: one-body row), active) into color[row_capacity],
+ * order[row_capacity] (rows stably sorted by color) and starts[129], and
+ * writes the color count to *num_colors (all device memory).  More than 128
+ * colors raise XPBD_ERR_OVERFLOW in *status_dev.  Temporary scratch;
+ * synchronizes the stream. */
+int xpbd_color_rows_device(int n_bodies, const int* row_i, const int* n_rows, int row_capacity, int* color,
+                           int* order, int* starts, int* num_colors, int* status_dev, void* stream);
 
 /* solver.py:275-342 _rebuild_contacts + solver.py:469-483 _sanitize_positions,
  * on the device.  Resets non-finite positions to x_init (float4[n]) with zero
@@ -166,9 +175,11 @@ int xpbd3_contacts_build(xpbd3_contacts* c, const xpbd3_state* s, const float* r
  * the frame kernel, captured once and replayed, with no host work between the
  * two.  Overflow and reset positions are reported through *status_dev only
  * (no per-frame host check).  The pointers must stay valid until the next
- * xpbd3_bind, which detaches, or until a call with c == NULL.  Jacobi only:
- * Gauss-Seidel colors the contact rows on the host every frame
- * (XPBD_ERR_BAD_ARG). */
+ * xpbd3_bind, which detaches, or until a call with c == NULL.  Gauss-Seidel:
+ * the frame also recolors the live rows on the device between the two
+ * (Welsh-Powell, coloring.py:26-89 and solver.py:396-397, bit-exact; the
+ * reference recolors on the host), into handle buffers of up to 128 colors;
+ * more colors raise XPBD_ERR_OVERFLOW in *status_dev. */
 int xpbd3_attach_contacts(xpbd3_solver* h, xpbd3_contacts* c, const float* radius, const float* friction,
                           const int* collide_idx, int n_collide, const int64_t* existing, int n_existing,
                           const float* x_init, double contact_margin, double dt, double r_max,

@@ -18,6 +18,7 @@
 #include <mutex>
 #include <vector>
 
+#include "coloring.cuh"
 #include "engine.cuh"
 
 namespace xpbd {
@@ -36,6 +37,7 @@ struct Dev3 {
   const int* cstarts;
   int n;
   int ncolors;
+  const int* ncolors_dev = nullptr;  // device color count (device-colored Gauss-Seidel frames), else ncolors
   float4* accs = nullptr;  // folded Jacobi: per-iteration accumulators, then the carry buffers (handle memory)
   int acc_stride = 0;
   // Gauss-Seidel on the cluster / grid drivers: the rows packed in color order
@@ -518,6 +520,9 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
   // visible (a no-op for an ordinary launch)
   asm volatile("griddepcontrol.wait;" ::: "memory");
   const int m = *g.n_rows;
+  // colors of this frame: written on the device by the coloring pass of a
+  // captured Gauss-Seidel frame with contacts, else fixed at bind
+  const int ncol = g.ncolors_dev ? *g.ncolors_dev : g.ncolors;
   Dev3 s = g;
   const bool packed = GS && SMEM && p.gs_packed;
   int2* prow = nullptr;
@@ -551,7 +556,7 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
         pval[k] = pv;
         s.lam[k] = g.lam[j];
       }
-      for (int c = threadIdx.x; c <= g.ncolors; c += blockDim.x) cst[c] = g.cstarts[c];
+      for (int c = threadIdx.x; c <= ncol; c += blockDim.x) cst[c] = g.cstarts[c];
     } else {
       for (int j = threadIdx.x; j < m; j += blockDim.x) s.lam[j] = g.lam[j];
     }
@@ -693,7 +698,7 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
       if (m > 0) {
         for (int it = 0; it < p.iterations; ++it) {
           if (GS && packed) {
-            for (int c = 0; c < g.ncolors; ++c) {
+            for (int c = 0; c < ncol; ++c) {
               const int start = cst[c], count = cst[c + 1] - start;
               for (int t = tid0; t < count; t += stride) {
                 const int k = start + t;
@@ -716,7 +721,7 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
           } else if (GS && gpk) {
             // kGsBatch rows of the color per step: their records, then all their
             // endpoints (rows of one color share no particle), then the projections
-            for (int c = 0; c < g.ncolors; ++c) {
+            for (int c = 0; c < ncol; ++c) {
               const int start = g.cstarts[c], count = g.cstarts[c + 1] - start;
               for (int t = tid0; t < count; t += kGsBatch * stride) {
                 int2 pr[kGsBatch];
@@ -760,7 +765,7 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
               sync();
             }
           } else if (GS) {
-            for (int c = 0; c < g.ncolors; ++c) {
+            for (int c = 0; c < ncol; ++c) {
               int start = g.cstarts[c], count = g.cstarts[c + 1] - start;
               for (int t = tid0; t < count; t += stride) {
                 int j = g.corder[start + t];
@@ -958,6 +963,13 @@ struct xpbd3_solver {
     int* status;
   } hook{};
   bool hooked = false;
+  // Gauss-Seidel with an attached contact rebuild: the rows are colored on the
+  // device every frame (k_color_rows) into these handle buffers
+  int* col_buf = nullptr;  // color[cap], order[cap], starts[kColMaxColors + 1], ncolors[1]
+  void* col_scratch = nullptr;
+  size_t col_bytes = 0, col_scratch_bytes = 0;
+  ColorArgs col{};
+  bool dev_color = false;
   cudaGraphExec_t graph = nullptr;
 };
 
@@ -1083,6 +1095,8 @@ extern "C" int xpbd3_destroy(xpbd3_solver* h) {
   free_graph3(h);
   if (h->bar) cudaFree(h->bar);
   if (h->accs) cudaFree(h->accs);
+  if (h->col_buf) cudaFree(h->col_buf);
+  if (h->col_scratch) cudaFree(h->col_scratch);
   delete h;
   return XPBD_OK;
 }
@@ -1103,6 +1117,7 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
   if (p->gs && s->row_capacity > 0 && (!s->color_order || !s->color_starts)) return XPBD_ERR_BAD_ARG;
   free_graph3(h);
   h->hooked = false;
+  h->dev_color = false;
   h->st = *s;
   h->par = *p;
   h->dev = make_dev3(s);
@@ -1229,6 +1244,7 @@ extern "C" int xpbd3_step(xpbd3_solver* h, int frames, void* stream) {
     }
     int rc = xpbd3_contacts_build(k.c, &h->st, k.radius, k.friction, k.coll, k.n_coll, k.existing, k.n_existing,
                                   k.x_init, k.margin, k.dt, k.rmax, k.status, cap);
+    if (!rc && h->dev_color) rc = color_rows_launch(h->col, cap);
     if (!rc) rc = run_frames(h, 1, cap, true);
     e = cudaStreamEndCapture(cap, &g);
     cudaStreamDestroy(cap);
@@ -1252,10 +1268,70 @@ extern "C" int xpbd3_attach_contacts(xpbd3_solver* h, xpbd3_contacts* c, const f
   if (!h) return XPBD_ERR_BAD_ARG;
   free_graph3(h);
   h->hooked = false;
+  if (h->dev_color) {
+    // back to the host-colored rows of the bound state
+    const xpbd3_state st = h->st;
+    const xpbd3_params par = h->par;
+    h->dev_color = false;
+    const int rc = xpbd3_bind(h, &st, &par);
+    if (rc) return rc;
+  }
   if (!c) return XPBD_OK;
-  if (h->par.gs || !radius || !friction || !x_init || !status_dev || n_collide < 0 || n_existing < 0 ||
+  if (!radius || !friction || !x_init || !status_dev || n_collide < 0 || n_existing < 0 ||
       (n_collide > 0 && !collide_idx) || (n_existing > 0 && !existing))
     return XPBD_ERR_BAD_ARG;
+  if (h->par.gs) {
+    // Gauss-Seidel: the rows change every frame, so they are colored on the
+    // device in the captured frame (k_color_rows), into handle buffers
+    const int n = h->st.n_bodies, cap = h->st.row_capacity;
+    if (n < 1 || cap < 1) return XPBD_ERR_BAD_ARG;
+    const size_t need = sizeof(int) * (2 * (size_t)cap + kColMaxColors + 2);
+    if (need > h->col_bytes) {
+      if (h->col_buf) cudaFree(h->col_buf);
+      h->col_buf = nullptr;
+      h->col_bytes = 0;
+      XPBD_CUDA(cudaMalloc(&h->col_buf, need));
+      h->col_bytes = need;
+    }
+    const size_t sb = color_scratch_bytes(n, cap);
+    if (sb > h->col_scratch_bytes) {
+      if (h->col_scratch) cudaFree(h->col_scratch);
+      h->col_scratch = nullptr;
+      h->col_scratch_bytes = 0;
+      XPBD_CUDA(cudaMalloc(&h->col_scratch, sb));
+      h->col_scratch_bytes = sb;
+    }
+    ColorArgs& A = h->col;
+    A = ColorArgs{};
+    A.ri = reinterpret_cast<const int4*>(h->st.row_i);
+    A.n_rows = h->st.n_rows;
+    A.n = n;
+    A.cap = cap;
+    A.color = h->col_buf;
+    A.order = h->col_buf + cap;
+    A.starts = h->col_buf + 2 * (size_t)cap;
+    A.ncolors = A.starts + kColMaxColors + 1;
+    A.status = status_dev;
+    color_scratch_carve(A, h->col_scratch, n, cap);
+    h->dev.corder = A.order;
+    h->dev.cstarts = A.starts;
+    h->dev.ncolors_dev = A.ncolors;
+    h->dev.ncolors = kColMaxColors;
+    if (h->mode == 1 && h->p3.gs_packed) {
+      // room for the color ranges of up to kColMaxColors colors
+      size_t packed = (size_t)n * 4 * sizeof(float4) + (size_t)cap * (sizeof(int2) + sizeof(float2) + sizeof(float)) +
+                      sizeof(int) * ((size_t)kColMaxColors + 1);
+      packed = (packed + 15) & ~(size_t)15;
+      if (packed <= kSmemMax) {
+        h->smem = packed;
+      } else {
+        h->p3.gs_packed = 0;
+        size_t sm = (size_t)n * 4 * sizeof(float4) + (size_t)cap * sizeof(float);
+        h->smem = (sm + 15) & ~(size_t)15;
+      }
+    }
+    h->dev_color = true;
+  }
   h->hook = {c, radius, friction, x_init, collide_idx, existing, n_collide, n_existing,
              contact_margin, dt, r_max, status_dev};
   h->hooked = true;

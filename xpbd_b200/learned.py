@@ -285,16 +285,25 @@ class WarmStartRunner:
     graph and replayed."""
 
     def __init__(self, s, model):
+        """`model`: a ``WarmStartMLP`` (learned lambda0) or ``"previous"`` (the
+        classical warm start: lambda0 = the previous substep's multipliers)."""
         if s.solve_mode != "jacobi":
             raise ValueError("the warm start drives the Jacobi solve")
+        if s._self_collision:
+            raise ValueError("the 3-DOF warm start needs fixed rows (the contact rows are rebuilt every frame)")
         self.s = s
         self.model = model
+        self.classic = isinstance(model, str)
+        if self.classic and model != "previous":
+            raise ValueError(f"unknown warm start {model!r}")
         self.kit = SubstepKit(s)
         T = s.tensors
         dev = s.device
         self.x_tilde = torch.empty_like(T["x"])
         self.x_plain = torch.empty_like(T["x"])
         self.lam_plain = torch.empty_like(T["lam"])
+        self.lam_prev = torch.empty_like(T["lam"])
+        self.binds = getattr(s, "binds", 0)
         self.res_p = torch.zeros(1, dtype=torch.float32, device=dev)
         self.res_l = torch.zeros(1, dtype=torch.float32, device=dev)
         self.learned_used = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -307,14 +316,20 @@ class WarmStartRunner:
     def _substep(self):
         kit, T = self.kit, self.s.tensors
         kit.integrate()
-        kit.features()
+        if self.classic:
+            self.lam_prev.copy_(T["lam"])
+        else:
+            kit.features()
         self.x_tilde.copy_(T["x"])
         kit.iterate(first=True)
         self._residual(self.res_p)
         self.x_plain.copy_(T["x"])
         self.lam_plain.copy_(T["lam"])
         T["x"].copy_(self.x_tilde)
-        kit.warm(self.model)
+        if self.classic:
+            kit.warm(lam0=self.lam_prev)
+        else:
+            kit.warm(self.model)
         kit.iterate(first=False)
         self._residual(self.res_l)
         use_plain = self.res_p <= self.res_l
@@ -604,3 +619,66 @@ def iterations_to_tol6(kit, model=None, tol=1e-4, max_iters=50, scale=1.0, varia
     kit.finish()
     kit.carry(lam_plain)
     return out
+
+
+class WarmStartRunner6:
+    """Steps a ``Solver6DOF`` frame with a warm-started contact solve, keeping
+    the plain lambda0 = 0 solve as the per-substep fallback (decided on the
+    device).
+
+    Per frame: the broad phase (the pair slots' previous multipliers follow
+    their pairs, ``SubstepKit6.broadphase``); per substep: integrate, manifold,
+    features; the first iteration plain, its residual; the same first iteration
+    from the same predicted state after the warm start, its residual; whichever
+    residual is smaller is kept (ties go to plain); the remaining iterations;
+    finalize and the velocity pass.  `model` is a ``WarmStartMLP`` (learned
+    lambda0) or ``"previous"`` (lambda0 = each row's multiplier over the
+    previous substep).  The same physics as the substep kernel otherwise."""
+
+    def __init__(self, s, model):
+        self.s = s
+        self.model = model
+        self.classic = isinstance(model, str)
+        if self.classic and model != "previous":
+            raise ValueError(f"unknown warm start {model!r}")
+        self.kit = SubstepKit6(s)
+        self.binds = getattr(s, "binds", 0)
+        dev = s.device
+        self.res_p = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.res_l = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.learned_used = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.substeps_run = 0
+
+    def _residual(self, out):
+        N.check(self.kit.L.xpbd6_residual(C.byref(self.s._st), C.byref(self.s._par), None, 1, N.ptr(out),
+                                          N.stream_of(self.s.device)), "xpbd6_residual")
+
+    def _substep(self):
+        kit, T = self.kit, self.s.tensors
+        kit.begin()
+        snap = kit.snapshot()
+        kit.iterate()
+        self._residual(self.res_p)
+        plain = (T["x"].clone(), T["q"].clone(), T["lam_floor"].clone(), T["lam_pair"].clone(),
+                 kit.tot_floor.clone())
+        kit.restore(snap)
+        if self.classic:
+            kit.warm(lam0=torch.cat([kit.prev_floor, kit.prev_pair]))
+        else:
+            kit.warm(self.model)
+        kit.iterate()
+        self._residual(self.res_l)
+        use_plain = self.res_p <= self.res_l
+        for cur, p in zip((T["x"], T["q"], T["lam_floor"], T["lam_pair"], kit.tot_floor), plain):
+            cur.copy_(torch.where(use_plain, p, cur))
+        self.learned_used += (~use_plain).to(torch.int32)
+        for _ in range(1, self.s.iterations):
+            kit.iterate()
+        kit.finish()
+        self.substeps_run += 1
+
+    def step(self):
+        self.kit.broadphase()  # may grow the pair capacity (a re-bind the kit has absorbed)
+        self.binds = getattr(self.s, "binds", 0)
+        for _ in range(self.s.substeps):
+            self._substep()

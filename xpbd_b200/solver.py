@@ -6,9 +6,12 @@ Host side: scene lists (as in the reference) are flushed to CUDA tensors in a
 packed float4 layout; a C-ABI handle (libxpbd_b200.so) then runs each frame as
 one persistent launch (``xpbd3_step``).  With self collision on, contacts are
 regenerated on the device every frame (``xpbd3_contacts_build``) in the
-reference's row order; in Gauss-Seidel mode the contact rows are then colored
-on the host with the same Welsh-Powell order as the reference, which (like the
-reference) costs one device-to-host round trip per frame.
+reference's row order.  In Gauss-Seidel mode the rows must then be recolored
+(Welsh-Powell, as the reference does on the host every frame): with
+``sync_contacts = False`` a one-CTA device pass colors them inside the frame's
+captured graph (contact rebuild + coloring + frame kernel); with
+``sync_contacts = True`` they are colored on the host after one
+device-to-host copy, with exact contact-capacity overflow handling.
 
 Differences from the reference, all deliberate:
 * ``device`` defaults to ``"cuda:0"``; a CPU device raises (the engine has no
@@ -48,8 +51,18 @@ class _Row:
 class Solver:
     def __init__(self, dt: float = 1.0 / 60.0, substeps: int = 10, iterations: int = 1,
                  gravity=(0.0, -9.81, 0.0), damping: float = 0.0, solve_mode: str = "auto",
-                 jacobi_relax: float = 1.0, device: str = "cuda:0", max_speed: float = 40.0):
+                 jacobi_relax: float = 1.0, device: str = "cuda:0", max_speed: float = 40.0, warm_start=None):
+        """As the reference's constructor, plus `warm_start` (no reference
+        counterpart; the reference restarts every substep from lambda = 0):
+        None (the reference's lambda0 = 0), ``"previous"`` (the classical warm
+        start from the previous substep's multipliers) or a
+        ``learned.WarmStartMLP`` (the learned lambda0).  A warm start drives
+        Jacobi solves of fixed rows (no self collision); every substep it also
+        runs the plain first iteration and keeps whichever first iteration
+        leaves the smaller residual."""
         self.device = N.require_cuda(device)
+        self.warm_start = warm_start
+        self._runner = None
         self.dt = float(dt)
         self.substeps = int(substeps)
         self.iterations = int(iterations)
@@ -355,9 +368,16 @@ class Solver:
             return
         L = N.lib()
         stream = N.stream_of(self.device)
+        if self.warm_start is not None:
+            if self._runner is None or self._runner.binds != self.binds:
+                from .learned import WarmStartRunner
+                self._runner = WarmStartRunner(self, self.warm_start)
+            self._runner.step()
+            return
         if self._self_collision:
-            if not self.sync_contacts and self.solve_mode != "gs":
-                # contact rebuild + frame kernel as one captured CUDA graph per bind
+            if not self.sync_contacts:
+                # contact rebuild (+ the device coloring of the rows, Gauss-Seidel)
+                # + frame kernel as one captured CUDA graph per bind
                 if not self._hooked:
                     self._attach_contacts(stream)
                 N.check(L.xpbd3_step(self._h, 1, stream), "xpbd3_step")

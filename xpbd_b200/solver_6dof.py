@@ -107,8 +107,17 @@ class Solver6DOF:
                  restitution: float = 0.0, lin_damp: float = 0.0, ang_damp: float = 0.0,
                  gyroscopic: bool = False, jacobi_relax: float = 1.0, device: str = "cuda:0",
                  max_speed: float = 60.0, max_omega: float = 60.0, broadphase: str = "lbvh",
-                 edge_axes: bool = False):
+                 edge_axes: bool = False, warm_start=None):
+        """As the reference's constructor, plus `edge_axes` (the nine edge-edge
+        SAT axes, off: the reference's manifold) and `warm_start` (no reference
+        counterpart; the reference zeroes the contact multipliers every
+        substep): None, ``"previous"`` (the classical warm start from each floor
+        corner's and manifold point's multiplier over the previous substep) or a
+        ``learned.WarmStartMLP``; a warm-started frame also runs the plain first
+        iteration every substep and keeps whichever leaves the smaller residual."""
         self.device = N.require_cuda(device)
+        self.warm_start = warm_start
+        self._runner = None
         self.dt = float(dt)
         self.substeps = int(substeps)
         self.iterations = int(iterations)
@@ -386,6 +395,12 @@ class Solver6DOF:
             self._bind()
         L = lib6()
         stream = N.stream_of(self.device)
+        if self.warm_start is not None:
+            if self._runner is None or self._runner.binds != self.binds:
+                from .learned import WarmStartRunner6
+                self._runner = WarmStartRunner6(self, self.warm_start)
+            self._runner.step()
+            return
         if not self.sync_pairs:
             N.check(L.xpbd6_step(self._h, 1, stream), "xpbd6_step")
             return
