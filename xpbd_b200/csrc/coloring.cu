@@ -182,7 +182,11 @@ __global__ void __launch_bounds__(kColThreads, 1) k_color_rows(ColorArgs A) {
 
 int color_rows_launch(const ColorArgs& A, cudaStream_t st) {
   const size_t smem = color_smem_bytes(A.n);
-  XPBD_CUDA(cudaFuncSetAttribute(k_color_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // The attribute is per function and shared by every handle's captured
+  // frame: raise it to the layout's largest size (kColSmemBodies bodies), never
+  // to this call's, so no smaller scene lowers the limit a larger one relies on.
+  XPBD_CUDA(cudaFuncSetAttribute(k_color_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)color_smem_bytes(kColSmemBodies)));
   k_color_rows<<<1, kColThreads, smem, st>>>(A);
   XPBD_LAUNCHED();
   return XPBD_OK;

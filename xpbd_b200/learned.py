@@ -397,6 +397,13 @@ class SubstepKit6:
         self.h = s.dt / s.substeps
         self._carry = None
         self._pair_prev = None
+        self.np_host = min(s.n_pairs, s.cap)
+        # manifold points summed over the substeps begun (the projection count)
+        self.points_dev = torch.zeros((), dtype=torch.int64, device=s.device)
+
+    @property
+    def points_total(self):
+        return int(self.points_dev.item())
 
     def _alloc(self):
         s, dev = self.s, self.s.device
@@ -448,6 +455,7 @@ class SubstepKit6:
             self.prev_floor.copy_(prev_floor)
         T = s.tensors
         n_new = min(s.n_pairs, self.cap)
+        self.np_host = n_new
         keys = T["pairs"][:n_new].long()
         keys = keys[:, 0] * self.n + keys[:, 1]
         mapped = torch.zeros((self.cap, 8), dtype=torch.float32, device=s.device)
@@ -476,6 +484,8 @@ class SubstepKit6:
             self._pair_prev = None
         N.check(self.L.xpbd6_integrate(self.st, self.par, self.stream()), "xpbd6_integrate")
         N.check(self.L.xpbd6_manifold(self.st, float(self.s._man_margin), self.stream()), "xpbd6_manifold")
+        if self.np_host:
+            self.points_dev += T["m_hdr"][: self.np_host, 0].sum()
         N.check(self.L.xpbd6_features(self.st, self.par, N.ptr(self.prev_floor), N.ptr(self.prev_pair),
                                       N.ptr(self.feats), N.ptr(self.weff), self.stream()), "xpbd6_features")
         self.tot_floor.zero_()

@@ -119,16 +119,24 @@ def evaluate_cloth(m, n=128, compliance=1e-5, frames=30, substeps=16, tol=1e-4, 
     s = make_cloth(n, compliance)
     for _ in range(frames):
         s.step()
-    rows = [iterations_to_tol(s, m, tol=tol, max_iters=max_iters, advance=True) for _ in range(substeps)][1:]
+    rows = [iterations_to_tol(s, m, tol=tol, max_iters=max_iters, advance=True, classic=True)
+            for _ in range(substeps)][1:]
     plain = np.array([r["plain"] for r in rows])
     learned = np.array([r["learned_with_fallback"] for r in rows])
+    classic = np.array([r["classic"] for r in rows])
     pf_plain = np.array([r["to_plain_final"]["plain"] for r in rows])
     pf_fb = np.array([r["to_plain_final"]["plain"] if r["fallback"] else r["to_plain_final"]["learned"] for r in rows])
     return {"scene": f"cloth {n}x{n}", "compliance": compliance, "tol_m": tol, "max_iters": max_iters,
             "substeps": len(rows), "iters_plain": plain.tolist(), "iters_learned": learned.tolist(),
             "fallbacks": int(sum(r["fallback"] for r in rows)),
             "mean_plain": float(plain.mean()), "mean_learned": float(learned.mean()),
+            "mean_classic": float(classic.mean()), "iters_classic": classic.tolist(),
             "ratio": float(plain.mean() / max(learned.mean(), 1e-9)),
+            "residual_first_iter_mean": {k: float(np.mean([r["residual_first_iter"][k] for r in rows]))
+                                         for k in ("plain", "learned", "classic")},
+            "residual_second_iter_mean": {
+                "plain": float(np.mean([r["residual_plain"][1] for r in rows])),
+                "learned": float(np.mean([r["residual_learned"][1] for r in rows]))},
             "iters_to_plain_final": {"plain": float(pf_plain.mean()), "learned_with_fallback": float(pf_fb.mean())},
             "plain_final_residual_mean": float(np.mean([r["residual_plain"][-1] for r in rows]))}
 
@@ -227,6 +235,53 @@ def time_warm_start(m):
     out["cloth"] = {"rows": rows3, "warm_start_ms": round(_event_ms(warm3), 4),
                     "iteration_ms": round(_event_ms(iter3), 4)}
     c.load_state_dict(snap3)
+    return out
+
+
+def product_frames(m, frames=20):
+    """Frames through the public ``step()`` with each ``warm_start`` setting on
+    the 128 x 128 cloth (compliance 1e-5, Jacobi) and the 1440-box pile (after
+    240 frames): ms per frame, M proj/s (rows x substeps x iterations; the
+    warm start's extra first iteration is overhead, not counted) and the mean
+    max residual after the frames."""
+    out = {}
+    for name in ("cloth", "pile"):
+        for label, ws in (("plain", None), ("previous", "previous"), ("learned", m)):
+            if name == "cloth":
+                s = Solver(dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi", warm_start=ws)
+                scenes.build_cloth(s, res=128, compliance=1e-5)
+                pre = 30
+            else:
+                s = Solver6DOF(device="cuda:0", warm_start=ws, **PILE_KW)
+                scenes.build_box_pile(s)
+                s.sync_pairs = False
+                pre = 240
+            for _ in range(pre):
+                s.step()
+            torch.cuda.synchronize()
+            if name == "pile":
+                s.manifold_points(reset=True)
+                n_dyn = int((s.tensors["x"][:, 3] > 0).sum().item())
+            res = []
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ms = 0.0
+            for _ in range(frames):
+                e0.record()
+                s.step()
+                e1.record()
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
+                res.append(float(np.max(s.residual())))
+            if name == "cloth":
+                proj = frames * s.num_constraints * s.substeps * s.iterations
+            else:
+                pts = s._runner.kit.points_total if ws is not None else s.manifold_points()
+                proj = s.iterations * (frames * s.substeps * (8 * n_dyn) + pts)
+            used = int(s._runner.learned_used.item()) if ws is not None else 0
+            out[f"{name}/{label}"] = {"ms_per_frame": round(ms / frames, 4),
+                                      "M_proj_per_s": round(proj / (ms / 1e3) / 1e6, 2),
+                                      "mean_max_residual": float(np.mean(res)),
+                                      "warm_substeps_kept": used}
     return out
 
 
