@@ -227,3 +227,50 @@ def test_shipped_weights_save_iterations_on_cloth():
     learned = np.mean([r["learned_with_fallback"] for r in rows])
     assert plain <= 150
     assert learned * 1.5 <= plain, (learned, plain)
+
+
+@pytest.mark.parametrize("ws", ["previous", "learned"])
+def test_warm_start_option_on_the_3dof_solver(ws):
+    """Solver(warm_start=...) steps through the public step(): frames stay
+    finite, the warm start is kept on most substeps of a hanging cloth, and the
+    residual after each frame is no worse than the plain solver's by more than
+    a few percent (both solve 2 iterations per substep)."""
+    model = WarmStartMLP.pretrained() if ws == "learned" else "previous"
+    kw = dict(dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi")
+    warm, plain = Solver(warm_start=model, **kw), Solver(**kw)
+    for s in (warm, plain):
+        scenes.build_cloth(s, res=24, compliance=1e-6)
+    for _ in range(12):
+        warm.step()
+        plain.step()
+    torch.cuda.synchronize()
+    assert np.all(np.isfinite(warm.positions()))
+    assert warm.status() == 0
+    kept = int(warm._runner.learned_used.item())
+    assert kept >= 0.5 * 12 * 15, kept
+    r_w, r_p = float(warm.residual()[0]), float(plain.residual()[0])
+    assert r_w <= 1.05 * r_p, (r_w, r_p)
+    with pytest.raises(ValueError):
+        s = Solver(warm_start="previous", **kw)
+        scenes.build_sphere_pile(s, nx=2, ny=2, nz=2)
+        s.step()
+
+
+@pytest.mark.parametrize("ws", ["previous", "learned"])
+def test_warm_start_option_on_the_6dof_solver(ws):
+    """Solver6DOF(warm_start=...) on a small settled pile: frames stay finite,
+    the pair list and positions track the plain solver's to the millimetre over
+    a few frames, and the device point count covers every substep."""
+    model = WarmStartMLP.pretrained() if ws == "learned" else "previous"
+    kw = dict(dt=1 / 60, substeps=15, iterations=2, floor_y=0.0, friction=0.6, restitution=0.2)
+    warm, plain = Solver6DOF(warm_start=model, **kw), Solver6DOF(**kw)
+    for s in (warm, plain):
+        scenes.build_box_pile(s, nx=3, ny=2, nz=3, pitch=0.7, y0=0.35)
+    for _ in range(20):
+        warm.step()
+        plain.step()
+    torch.cuda.synchronize()
+    assert np.all(np.isfinite(warm.positions())) and np.all(np.isfinite(warm.orientations()))
+    assert warm.status() == 0
+    assert np.abs(warm.positions() - plain.positions()).max() < 0.05
+    assert warm._runner.kit.points_total > 0

@@ -313,6 +313,7 @@ def main():
     report["cloth_c1e-4"] = evaluate_cloth(m, compliance=1e-4)
     report["pile"] = evaluate_pile(m)
     report["timing"] = time_warm_start(m)
+    report["frames"] = product_frames(m)
     print(json.dumps(report))
 
 
