@@ -127,6 +127,12 @@ int xpbd3_set_driver(xpbd3_solver* h, int mode, int blocks, int threads);
 /* Barriers and phases (work between barriers) of one frame of the bound frame
  * kernel (no reference counterpart; the benchmark's latency model). */
 int xpbd3_phases(xpbd3_solver* h, int* barriers, int* phases);
+/* The bound rows' parameters (row_f, row_anchor, row_i's active flags) were
+ * edited in place (no reference counterpart; the reference re-flushes every
+ * array): Gauss-Seidel launches on the cluster / grid drivers keep the rows
+ * packed in color order across launches and pack them again after this call
+ * (asynchronous on `stream`).  A bind always repacks. */
+int xpbd3_rows_changed(xpbd3_solver* h, void* stream);
 
 /* Constraint residual after a solve (no reference counterpart; the metric of
  * the benchmark and of the learned warm start): hard rows max(0, -C),

@@ -408,3 +408,27 @@ def test_captured_frame_reports_contact_overflow():
     assert s.status() & N.XPBD_ERR_OVERFLOW
     assert s.num_constraints == len(s.rows()["type"]) <= s._cap
     assert np.all(np.isfinite(s.positions()))
+
+
+def test_gs_packed_rows_follow_the_setters():
+    """Gauss-Seidel on the grid driver keeps its rows packed in color order
+    across launches and packs them again after a setter: frames before and
+    after set_all_compliance / set_all_friction agree bit for bit with the
+    one-CTA driver, which stages the rows afresh in every launch."""
+    out = []
+    for drv in ((0, 4, 256), (1, 0, 0)):
+        s = Solver(device="cuda:0", dt=1 / 60, substeps=15, iterations=2, solve_mode="gs")
+        scenes.build_cloth(s, res=16, spacing=0.03, y=0.05, velocity=(0.1, -0.5, 0.0))
+        s.set_driver(*drv)
+        for _ in range(3):
+            s.step()
+        binds = s.binds
+        s.set_all_compliance(1e-5)
+        s.set_all_friction(0.05)
+        for _ in range(3):
+            s.step()
+        assert s.binds == binds
+        out.append((s.launch_info()["mode"], s.positions(), s.lambdas()))
+    assert out[0][0] == "grid" and out[1][0] == "shared"
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    np.testing.assert_array_equal(out[0][2], out[1][2])

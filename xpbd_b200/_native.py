@@ -87,6 +87,7 @@ _SIGS = {
     "xpbd_barrier_selftest": ([C.c_int, C.c_int, C.c_int, _p, _p], C.c_int),
     "xpbd_phase_floor": ([C.c_int, C.c_int, C.c_int, C.c_int, _p, _p], C.c_int),
     "xpbd3_phases": ([_p, _ip, _ip], C.c_int),
+    "xpbd3_rows_changed": ([_p, _p], C.c_int),
     "xpbd_color_rows_device": ([C.c_int, _p, _p, C.c_int, _p, _p, _p, _p, _p, _p], C.c_int),
     "xpbd6_phases": ([_p, _ip, _ip], C.c_int),
     "xpbd3_attach_contacts": ([_p, _p, _p, _p, _p, C.c_int, _p, C.c_int, _p, C.c_double, C.c_double,

@@ -45,6 +45,7 @@ struct Dev3 {
   int2* gprow = nullptr;
   float2* gpval = nullptr;
   float* glam = nullptr;
+  int* pack_flag = nullptr;  // nonzero: pack the rows again (handle memory)
 };
 
 struct Par3 {
@@ -54,6 +55,7 @@ struct Par3 {
   int carry = 0;  // 1 (with fold): the substep boundary folded into the first iteration's reads too
   int gs_packed = 0;   // 1 (Gauss-Seidel, one CTA): the rows staged in shared memory in color order
   int gs_gpacked = 0;  // 1 (Gauss-Seidel, cluster / grid): the rows packed in color order in global memory
+  int pack_always = 0; // 1: pack the rows in every launch (captured frames that rebuild them)
 };
 
 // ---------------------------------------------------------------------------
@@ -605,7 +607,13 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
   // stores the frame state.
   const bool carry_path = !GS && !SMEM && p.fold && p.carry && m > 0;
   const bool gpk = GS && !SMEM && p.gs_gpacked && m > 0;
-  if (gpk) {
+  // The rows packed in color order stay valid across launches: they are packed
+  // again only when a bind or a row setter (xpbd3_rows_changed) has raised the
+  // handle's flag, or in every launch of a captured frame that rebuilds its
+  // rows (pack_always).  Every CTA reads the flag before the barrier after the
+  // packing, and only then does CTA 0 clear it.  The packed multipliers need
+  // no copy: the first iteration of every substep starts them from 0.
+  if (gpk && (p.pack_always || *g.pack_flag != 0)) {
     for (int k = tid0; k < m; k += stride) {
       const int j = g.corder[k];
       int2 pr;
@@ -613,9 +621,9 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
       pack_gs_row(g.ri[j], g.rf[j], j, pr, pv);
       g.gprow[k] = pr;
       g.gpval[k] = pv;
-      g.glam[k] = g.lam[j];
     }
     sync();
+    if (tid0 == 0 && !p.pack_always) *g.pack_flag = 0;
   }
   auto rows_first = [&](const auto& pos, const AccGlobal& acc) {
     if (cache_rows) {
@@ -1079,13 +1087,14 @@ static int configure(xpbd3_solver* h) {
 extern "C" int xpbd3_create(xpbd3_solver** out) {
   if (!out) return XPBD_ERR_BAD_ARG;
   xpbd3_solver* h = new xpbd3_solver();
-  cudaError_t e = cudaMalloc(&h->bar, 4 * sizeof(unsigned));
+  // words 0-3: the grid barrier (count, status, exits); 4: the Gauss-Seidel repack flag
+  cudaError_t e = cudaMalloc(&h->bar, 8 * sizeof(unsigned));
   if (e != cudaSuccess) {
     set_last_error("cudaMalloc", e);
     delete h;
     return XPBD_ERR_CUDA;
   }
-  cudaMemset(h->bar, 0, 4 * sizeof(unsigned));
+  cudaMemset(h->bar, 0, 8 * sizeof(unsigned));
   *out = h;
   return XPBD_OK;
 }
@@ -1208,6 +1217,8 @@ extern "C" int xpbd3_bind(xpbd3_solver* h, const xpbd3_state* s, const xpbd3_par
     h->dev.gprow = reinterpret_cast<int2*>(h->accs);
     h->dev.gpval = reinterpret_cast<float2*>(h->dev.gprow + cap);
     h->dev.glam = reinterpret_cast<float*>(h->dev.gpval + cap);
+    h->dev.pack_flag = reinterpret_cast<int*>(h->bar + 4);
+    XPBD_CUDA(cudaMemset(h->bar + 4, 1, 1));  // new rows or colors: pack at the next launch
     q.gs_gpacked = 1;
   }
   int rc;
@@ -1245,7 +1256,9 @@ extern "C" int xpbd3_step(xpbd3_solver* h, int frames, void* stream) {
     int rc = xpbd3_contacts_build(k.c, &h->st, k.radius, k.friction, k.coll, k.n_coll, k.existing, k.n_existing,
                                   k.x_init, k.margin, k.dt, k.rmax, k.status, cap);
     if (!rc && h->dev_color) rc = color_rows_launch(h->col, cap);
+    h->p3.pack_always = 1;  // the rows change every frame
     if (!rc) rc = run_frames(h, 1, cap, true);
+    h->p3.pack_always = 0;
     e = cudaStreamEndCapture(cap, &g);
     cudaStreamDestroy(cap);
     if (rc) {
@@ -1347,6 +1360,14 @@ extern "C" int xpbd3_status(xpbd3_solver* h, int* out, void* stream) {
   return XPBD_OK;
 }
 
+// Row parameters edited in place (the setters): Gauss-Seidel launches on the
+// cluster / grid drivers pack the rows in color order again at their start.
+extern "C" int xpbd3_rows_changed(xpbd3_solver* h, void* stream) {
+  if (!h) return XPBD_ERR_BAD_ARG;
+  XPBD_CUDA(cudaMemsetAsync(h->bar + 4, 1, 1, as_stream(stream)));
+  return XPBD_OK;
+}
+
 // Barriers and phases of one frame of k3_frames as bound (the same conditions
 // the kernel tests; the live row count is taken as nonzero when rows exist).
 // A phase is the work between two barriers; the folded-boundary path ends with
@@ -1362,7 +1383,7 @@ extern "C" int xpbd3_phases(xpbd3_solver* h, int* barriers, int* phases) {
     b = (long long)S * I;
     ph = b + 1;
   } else {
-    b = 1 + ((q.gs && !smem && q.gs_gpacked && rows) ? 1 : 0);
+    b = 1 + ((q.gs && !smem && q.gs_gpacked && rows && h->hooked) ? 1 : 0);  // repacked every frame
     long long per_sub = 1;
     if (rows) {
       if (q.gs) per_sub += (long long)I * h->dev.ncolors;

@@ -164,6 +164,7 @@ class Solver:
         rt = self._t["row_i"][: len(self._rows), 0]
         sel = (rt == DISTANCE) if only_distance else torch.ones_like(rt, dtype=torch.bool)
         self._t["row_f"][: len(self._rows), 1][sel] = float(value)
+        self.rows_changed()
 
     def set_all_friction(self, mu: float) -> None:
         self._flush()
@@ -177,6 +178,14 @@ class Solver:
         self._t["row_f"][:, 2][(rt == FLOOR) | (rt == CONTACT)] = float(mu)
         if "friction" in self._t:
             self._t["friction"].fill_(float(mu))
+        self.rows_changed()
+
+    def rows_changed(self) -> None:
+        """Row parameters were edited in place on the device (the setters above,
+        or a caller writing ``tensors["row_f"]``): Gauss-Seidel frames pack the
+        rows in color order again before their next launch."""
+        self._flush()
+        N.check(N.lib().xpbd3_rows_changed(self._h, N.stream_of(self.device)), "xpbd3_rows_changed")
 
     # ---- flush: host lists -> device tensors (solver.py:346-408) -------------------
     def _flush(self) -> None:
