@@ -254,7 +254,6 @@ def time_batch(args, device, flush_buf, clocks=None, rank=0, world=1, n_scenes=2
     frame_ms = [a.elapsed_time(c) for a, c in ev]
     proj_total = b.projections(args.steps)
     points_total = b.piles.manifold_points() if b.has_piles else 0
-    res = b.residuals()
     frames_done = args.warmup + args.steps
     # per-kernel time on further frames (each system alone, L2 flushed), for the roofline
     S, I = b.cloth.substeps, b.cloth.iterations
@@ -272,6 +271,7 @@ def time_batch(args, device, flush_buf, clocks=None, rank=0, world=1, n_scenes=2
         torch.cuda.synchronize(device)
         kern[name] = statistics.mean(a.elapsed_time(c) for a, c in kev)
     frames_done += 5
+    res = b.residuals()  # after every frame the solo runs below repeat
     checks = {}
     for i in sample:
         if i not in b.scene_ids:

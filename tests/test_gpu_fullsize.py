@@ -40,8 +40,11 @@ def test_one_substep_sphere_pile_2048_settled():
     kw = dict(dt=H, substeps=1, iterations=2, solve_mode="jacobi")
     eng = Solver(device="cuda:0", **kw)
     orc = O.OracleSolver(device="cpu", **kw)
-    scenes.build_sphere_pile(eng)
-    scenes.build_sphere_pile(orc)
+    # a 5 mm contact margin: every pair of resting neighbours gets a row (the
+    # settled spheres touch within float rounding, so without a margin only the
+    # pairs that happen to overlap do)
+    scenes.build_sphere_pile(eng, margin=0.005)
+    scenes.build_sphere_pile(orc, margin=0.005)
     eng._flush()
     _seed3(eng, orc, x, v)
     for k in range(3):
@@ -54,7 +57,7 @@ def test_one_substep_sphere_pile_2048_settled():
         m = len(orc._rows)
         assert len(rows["type"]) == m
         n_contacts = int((rows["type"] == 3).sum())
-        assert n_contacts > 1000, n_contacts  # a settled, contact-rich pile
+        assert n_contacts > 2000, n_contacts  # a settled, contact-rich pile
         np.testing.assert_array_equal(rows["type"], orc.r_type)
         np.testing.assert_array_equal(rows["a"], orc.r_a)
         np.testing.assert_array_equal(rows["b"], orc.r_b)
