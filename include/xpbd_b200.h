@@ -225,6 +225,10 @@ int xpbd_mlp_grads(const float* feats, const float* targets, int B, const void* 
                    float* loss, void* stream);
 /* One Adam step on fp32 master weights w (moments M, V); refreshes the bf16 copy, clears G. */
 int xpbd_mlp_adam(float* w, float* G, float* M, float* V, void* weights_bf16, float lr, int step, void* stream);
+/* One training step on a batch: xpbd_mlp_grads (G must hold zeros) then
+ * xpbd_mlp_adam; *loss (device) receives the batch loss. */
+int xpbd_mlp_train_step(const float* feats, const float* targets, int B, float* w, float* G, float* M, float* V,
+                        void* weights_bf16, float lr, int step, float* loss, void* stream);
 /* Seeds lambda := lambda0 and accumulates the Jacobi position correction
  * M^-1 grad C^T lambda0 into acc (apply with xpbd3_apply_jacobi). */
 int xpbd3_warm_start(const xpbd3_state* s, const float* lam0, void* stream);

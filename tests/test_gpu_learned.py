@@ -61,6 +61,28 @@ def test_mlp_inference_matches_oracle():
     np.testing.assert_allclose(lam0.cpu().numpy(), ref, rtol=1e-4, atol=1e-9)
 
 
+def test_train_step_entry_point_equals_grads_then_adam():
+    """xpbd_mlp_train_step through the C ABI: the same weights, bit for bit, as
+    xpbd_mlp_grads followed by xpbd_mlp_adam."""
+    from xpbd_b200 import _native as N
+    rng = np.random.default_rng(2)
+    feats = torch.from_numpy(rng.normal(size=(700, 8)).astype(np.float32)).cuda()
+    targets = torch.from_numpy(rng.normal(size=700).astype(np.float32)).cuda()
+    a, b = WarmStartMLP(seed=9), WarmStartMLP(seed=9)
+    for step in (1, 2):
+        a.train_step(feats, targets, lr=1e-3)
+        loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        fn = N.lib().xpbd_mlp_train_step
+        fn.argtypes = [C.c_void_p] * 8 + [C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+        fn.restype = C.c_int
+        N.check(fn(N.ptr(feats), N.ptr(targets), 700, N.ptr(b.w), N.ptr(b.G), N.ptr(b.M), N.ptr(b.V), N.ptr(b.wb),
+                   1e-3, step, N.ptr(loss), N.stream_of("cuda:0")), "xpbd_mlp_train_step")
+        torch.cuda.synchronize()
+        assert float(loss.item()) > 0.0
+    np.testing.assert_array_equal(a.w.cpu().numpy(), b.w.cpu().numpy())
+    np.testing.assert_array_equal(a.wb.float().cpu().numpy(), b.wb.float().cpu().numpy())
+
+
 def _cloth(res=32, compliance=1e-5):
     """A hanging 32 x 32 cloth (spacing 0.02 m, 0.01 kg) at a compliance where
     the plain Jacobi solve does reach 1e-4 m, slowly (a stiffer cloth never

@@ -337,6 +337,15 @@ extern "C" int xpbd_mlp_adam(float* w, float* G, float* M, float* V, void* weigh
   return XPBD_OK;
 }
 
+// One training step: the batch gradient (added into G) then the Adam update,
+// which clears G and refreshes the bf16 copy the inference reads.
+extern "C" int xpbd_mlp_train_step(const float* feats, const float* targets, int B, float* w, float* G, float* M,
+                                   float* V, void* weights_bf16, float lr, int step, float* loss, void* stream) {
+  const int rc = xpbd_mlp_grads(feats, targets, B, weights_bf16, G, loss, stream);
+  if (rc) return rc;
+  return xpbd_mlp_adam(w, G, M, V, weights_bf16, lr, step, stream);
+}
+
 extern "C" int xpbd3_warm_start(const xpbd3_state* s, const float* lam0, void* stream) {
   if (!s || !lam0 || !s->acc || !s->n_rows) return XPBD_ERR_BAD_ARG;
   if (s->row_capacity == 0) return XPBD_OK;
