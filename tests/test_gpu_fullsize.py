@@ -1,5 +1,6 @@
 """One substep on identical state at the benchmark sizes: the 2048-sphere pile
-after 60 frames and the 1440-box pile after 100 frames, both contact-rich.
+at its contact-richest frame of the first 60 (while it lands) and the 1440-box
+pile after 100 frames.
 
 The settled state comes from the engine.  Then an engine and an oracle solver
 with one substep per frame (dt = h = 1/900 s, the same 2 iterations) are both
@@ -34,9 +35,16 @@ def _seed3(eng, orc, x, v):
 def test_one_substep_sphere_pile_2048_settled():
     settle = Solver(device="cuda:0", dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi")
     scenes.build_sphere_pile(settle)
+    # The pile lands after about 0.4 s and then spreads out over the floor (an
+    # averaged-Jacobi stack of spheres does not stand), so its contact count
+    # peaks while it lands: take the contact-richest of the first 60 frames.
+    best = (-1, None, None)
     for _ in range(60):
         settle.step()
-    x, v = settle.positions(), settle.velocities()
+        n_c = settle.num_constraints - settle.num_bodies
+        if n_c > best[0]:
+            best = (n_c, settle.positions(), settle.velocities())
+    _, x, v = best
     kw = dict(dt=H, substeps=1, iterations=2, solve_mode="jacobi")
     eng = Solver(device="cuda:0", **kw)
     orc = O.OracleSolver(device="cpu", **kw)

@@ -60,31 +60,30 @@ XD uint64_t global_ns() {
 // kernel can never hang on it.  With one block it is a plain __syncthreads().
 // Grid-wide barrier of a cooperative launch (or the hardware barrier when the
 // grid is one thread-block cluster).  The software form is a ticket barrier:
-// the arrival count (64 bits) only grows, every CTA arrives once at every
-// barrier, so a barrier completes when the count reaches the next multiple of
-// the grid size -- one release atomic per CTA and acquire polls, no reset on
-// the critical path.  Every CTA calls grid_exit at the end of the kernel; the
-// last one resets the count, so each launch starts from zero whatever grid
-// size it has.  Words: [0..1] count, [2] status, [3] exits.
+// the arrival count (64 bits) only grows, and every CTA arrives once at every
+// barrier.  Each launch starts from zero (every CTA calls grid_exit at the end
+// of the kernel, and the last one resets the count), so barrier k of a launch
+// completes when the count reaches k x the grid size: thread 0 of each CTA
+// keeps k x the grid size in `epoch` (its own copy of the barrier argument),
+// arrives with one fire-and-forget gpu-scope release reduction and polls with
+// acquire loads.  No arrival waits for an atomic's return value before it
+// polls, so the last CTA to arrive sees the barrier complete one L2 round trip
+// after its arrival.  Words: [0..1] count, [2] status, [3] exits.
 struct GridBarrier {
   unsigned long long* count;
   int* status;
   unsigned* exits;
   int cluster;  // 1: the grid is one thread-block cluster -> hardware cluster barrier
+  unsigned long long epoch;  // (thread 0 of each CTA) the count that completes the last barrier passed
 };
 
 inline GridBarrier make_grid_barrier(unsigned* words, int cluster) {
   return GridBarrier{reinterpret_cast<unsigned long long*>(words), reinterpret_cast<int*>(words + 2), words + 3,
-                     cluster};
+                     cluster, 0ull};
 }
 
 constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;
 
-XD unsigned long long atom_add_release_gpu(unsigned long long* p, unsigned long long v) {
-  unsigned long long old;
-  asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
-  return old;
-}
 XD int atom_add_acq_rel_gpu(int* p, int v) {
   int old;
   asm volatile("atom.add.acq_rel.gpu.global.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
@@ -96,7 +95,11 @@ XD unsigned long long ld_acquire_gpu(const unsigned long long* p) {
   return v;
 }
 
-XD void grid_sync(const GridBarrier& b) {
+XD void red_add_release_gpu(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+XD void grid_sync(GridBarrier& b) {
   if (gridDim.x == 1) {
     __syncthreads();
     return;
@@ -114,9 +117,9 @@ XD void grid_sync(const GridBarrier& b) {
   // the CTA (a base-causality chain of the PTX memory model).
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned long long N = gridDim.x;
-    const unsigned long long prev = atom_add_release_gpu(b.count, 1ull);
-    const unsigned long long target = prev - prev % N + N;
+    b.epoch += gridDim.x;
+    const unsigned long long target = b.epoch;
+    red_add_release_gpu(b.count, 1ull);
     volatile int* vstat = b.status;
     uint64_t t0 = 0;
     unsigned spins = 0;

@@ -685,6 +685,14 @@ class WarmStartRunner6:
         for _ in range(1, self.s.iterations):
             kit.iterate()
         kit.finish()
+        # A floor corner's impulse is carried only while the corner is still in
+        # contact after the last iteration.  The floor solve assigns its
+        # multiplier and only pushes (kernels_6dof.py:185-193): a carried impulse
+        # that lifted the corner off the floor would otherwise be applied again
+        # every substep, with nothing to take it back, and pump energy into the
+        # body.  (Manifold points need no mask: a separated point's multiplier
+        # is already set to 0 by its solve.)
+        kit.prev_floor.mul_((T["lam_floor"][: kit.nf] != 0).to(kit.prev_floor.dtype))
         self.substeps_run += 1
 
     def step(self):
