@@ -658,8 +658,6 @@ class WarmStartRunner6:
         self.res_l = torch.zeros(1, dtype=torch.float32, device=dev)
         self.learned_used = torch.zeros(1, dtype=torch.int32, device=dev)
         self.substeps_run = 0
-        self.scale = 1.0  # lambda0 := scale * the start (damped carry of the contacts' impulses)
-        self.mask = True  # carry a floor corner's impulse only while it stays in contact
 
     def _residual(self, out):
         N.check(self.kit.L.xpbd6_residual(C.byref(self.s._st), C.byref(self.s._par), None, 1, N.ptr(out),
@@ -675,9 +673,9 @@ class WarmStartRunner6:
                  kit.tot_floor.clone())
         kit.restore(snap)
         if self.classic:
-            kit.warm(scale=self.scale, lam0=torch.cat([kit.prev_floor, kit.prev_pair]))
+            kit.warm(lam0=torch.cat([kit.prev_floor, kit.prev_pair]))
         else:
-            kit.warm(self.model, scale=self.scale)
+            kit.warm(self.model)
         kit.iterate()
         self._residual(self.res_l)
         use_plain = self.res_p <= self.res_l
@@ -688,14 +686,12 @@ class WarmStartRunner6:
             kit.iterate()
         kit.finish()
         # A floor corner's impulse is carried only while the corner is still in
-        # contact after the last iteration.  The floor solve assigns its
-        # multiplier and only pushes (kernels_6dof.py:185-193): a carried impulse
-        # that lifted the corner off the floor would otherwise be applied again
-        # every substep, with nothing to take it back, and pump energy into the
-        # body.  (Manifold points need no mask: a separated point's multiplier
-        # is already set to 0 by its solve.)
-        if self.mask:
-            kit.prev_floor.mul_((T["lam_floor"][: kit.nf] != 0).to(kit.prev_floor.dtype))
+        # contact after the last iteration: the floor solve assigns its
+        # multiplier and only pushes (kernels_6dof.py:185-193), so the substep
+        # total of a corner that has lifted off is no estimate of the next
+        # substep's.  (A separated manifold point's multiplier is already set
+        # to 0 by its solve.)
+        kit.prev_floor.mul_((T["lam_floor"][: kit.nf] != 0).to(kit.prev_floor.dtype))
         self.substeps_run += 1
 
     def step(self):
