@@ -721,31 +721,9 @@ XD int gscan_ex(const Grp& G, int v, int* total) {  // exclusive prefix within t
   return inc - v;
 }
 
-// A lane group's records of its first pair or floor body in a substep, kept in
-// shared memory across the substep's phases (k6_substeps8): the manifold the
-// group generated, each lane's multiplier, and body records fetched ahead of
-// the phase that needs them.  pre: pair -> x, q, inv_I of the incident body,
-// then of the reference body; floor body -> x, q, he, inv_I, x_prev, q_prev.
-struct GroupCache {
-  int4 hdr;  // manifold count, incident, reference
-  float4 nrm;
-  float4 off_inc[8], off_ref[8];
-  float4 pre[6];
-  float lam[8];  // this lane's pair slot or floor corner multiplier
-  int2 ab;       // the pair's bodies (fixed for the launch)
-  int pad[2];
-};
-
-XD void cp_async16(void* smem_dst, const void* gmem_src) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem_src) : "memory");
-}
-XD void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// kernels_6dof.py:159-211 on eight lanes, from the body's records; lam_cache
-// (shared memory, or null) mirrors every write of the lane's multiplier.
-XD void floor_body8_core(const Dev6& s, int i, const Par6& p, const Grp& G, float4 x4, float4 q4i, float4 he4,
-                         float4 I4, float4 xp4, float4 qp4, float* lam_cache) {
+XD void floor_body8(const Dev6& s, int i, const Par6& p, const Grp& G) {
+  // every load first (one round trip), then the arithmetic
+  const float4 x4 = s.x[i], q4i = s.q[i], he4 = s.he[i], I4 = s.inv_I[i], xp4 = s.xp[i], qp4 = s.qp[i];
   float im = x4.w;
   if (im == 0.0f) return;
   V3 xi = v3(x4), he = v3(he4), Ii = v3(I4);
@@ -762,14 +740,12 @@ XD void floor_body8_core(const Dev6& s, int i, const Par6& p, const Grp& G, floa
   const int slot = 8 * i + c;
   if (d <= 0.0f) {
     s.lam_floor[slot] = 0.0f;
-    if (lam_cache) *lam_cache = 0.0f;
   } else {
     V3 r = p1 - xi;
     float wg = gen_inv_mass(im, qi, Ii, r, S);
     if (wg > 0.0f) {
       float dlam = d / wg;
       s.lam_floor[slot] = dlam;
-      if (lam_cache) *lam_cache = dlam;
       V3 P = S * dlam;
       dx = P * im;
       dr = world_invI_mul(qi, Ii, cross(r, P));
@@ -799,41 +775,21 @@ XD void floor_body8_core(const Dev6& s, int i, const Par6& p, const Grp& G, floa
   }
 }
 
-XD void floor_body8(const Dev6& s, int i, const Par6& p, const Grp& G) {
-  // every load first (one round trip), then the arithmetic
-  const float4 x4 = s.x[i], q4i = s.q[i], he4 = s.he[i], I4 = s.inv_I[i], xp4 = s.xp[i], qp4 = s.qp[i];
-  floor_body8_core(s, i, p, G, x4, q4i, he4, I4, xp4, qp4, nullptr);
-}
-
-// The group's cached floor body: the first iteration reads every record from
-// the prefetch (landed during the previous barrier), later ones reload the pose.
-XD void floor_body8_cached(const Dev6& s, int i, const Par6& p, const Grp& G, GroupCache& gc, bool prefetched) {
-  float4 x4, q4i;
-  if (prefetched) {
-    cp_async_wait_all();
-    __syncwarp(G.mask);
-    x4 = gc.pre[0];
-    q4i = gc.pre[1];
-  } else {
-    x4 = s.x[i];
-    q4i = s.q[i];
-  }
-  floor_body8_core(s, i, p, G, x4, q4i, gc.pre[2], gc.pre[3], gc.pre[4], gc.pre[5], &gc.lam[G.l]);
-}
-
-// kernels_6dof.py:386-430 on eight lanes (a lane per manifold point), from the
-// pair's records; returns the pair's manifold point count.
-XD int box_pair8_core(const Dev6& s, int pid, const Grp& G, int4 hdr, float4 nrm, float4 off_inc, float4 off_ref,
-                      float lam_slot, float4 xi4, float4 qi4, float4 Ii4, float4 xr4, float4 qr4, float4 Ir4,
-                      float* lam_cache) {
+XD int box_pair8(const Dev6& s, int pid, const Grp& G) {  // returns the pair's manifold point count
+  // the pair's own records with the header (one round trip), the bodies next
   const int c = G.l;
   const int slot = 8 * pid + c;
+  int4 hdr = s.m_hdr[pid];
+  const float4 nrm = s.m_normal[pid], off_inc = s.m_off_inc[slot], off_ref = s.m_off_ref[slot];
+  const float lam_slot = s.lam_pair[slot];
   const int nc = hdr.x;
+  if (nc == 0) return 0;
   const int inc = hdr.y, ref = hdr.z;
   V3 S = v3(nrm);
+  float4 xi4 = s.x[inc], xr4 = s.x[ref];
   V3 xi = v3(xi4), xr = v3(xr4);
-  Q4 qi = q4(qi4), qr = q4(qr4);
-  V3 Ii = v3(Ii4), Ir = v3(Ir4);
+  Q4 qi = q4(s.q[inc]), qr = q4(s.q[ref]);
+  V3 Ii = v3(s.inv_I[inc]), Ir = v3(s.inv_I[ref]);
   const float imi = xi4.w, imr = xr4.w;
   V3 dxi = V3{0, 0, 0}, dri = V3{0, 0, 0}, dxr = V3{0, 0, 0}, drr = V3{0, 0, 0};
   float ci = 0.0f, cr = 0.0f;
@@ -843,7 +799,6 @@ XD int box_pair8_core(const Dev6& s, int pid, const Grp& G, int4 hdr, float4 nrm
     float C = dot(p_inc - p_ref, S);
     if (C >= 0.0f) {
       s.lam_pair[slot] = 0.0f;
-      if (lam_cache) *lam_cache = 0.0f;
     } else {
       float d = -C;
       V3 r_inc = p_inc - xi, r_ref = p_ref - xr;
@@ -853,7 +808,6 @@ XD int box_pair8_core(const Dev6& s, int pid, const Grp& G, int4 hdr, float4 nrm
       if (wsum > 0.0f) {
         float dlam = d / wsum;
         s.lam_pair[slot] = lam_slot + dlam;
-        if (lam_cache) *lam_cache = lam_slot + dlam;
         V3 P = S * dlam;
         if (imi > 0.0f) {
           dxi = P * imi;
@@ -887,48 +841,11 @@ XD int box_pair8_core(const Dev6& s, int pid, const Grp& G, int4 hdr, float4 nrm
   return nc;
 }
 
-XD int box_pair8(const Dev6& s, int pid, const Grp& G) {  // returns the pair's manifold point count
-  // the pair's own records with the header (one round trip), the bodies next
-  const int slot = 8 * pid + G.l;
-  int4 hdr = s.m_hdr[pid];
-  const float4 nrm = s.m_normal[pid], off_inc = s.m_off_inc[slot], off_ref = s.m_off_ref[slot];
-  const float lam_slot = s.lam_pair[slot];
-  if (hdr.x == 0) return 0;
-  const int inc = hdr.y, ref = hdr.z;
-  return box_pair8_core(s, pid, G, hdr, nrm, off_inc, off_ref, lam_slot, s.x[inc], s.q[inc], s.inv_I[inc], s.x[ref],
-                        s.q[ref], s.inv_I[ref], nullptr);
-}
-
-// The group's cached pair: the manifold and multipliers from shared memory, the
-// bodies from the prefetch in the first iteration (landed during the previous
-// barrier), their poses reloaded in later ones.
-XD int box_pair8_cached(const Dev6& s, int pid, const Grp& G, GroupCache& gc, bool prefetched) {
-  const int4 hdr = gc.hdr;
-  if (hdr.x == 0) return 0;
-  float4 xi4, qi4, xr4, qr4;
-  if (prefetched) {
-    cp_async_wait_all();
-    __syncwarp(G.mask);
-    xi4 = gc.pre[0];
-    qi4 = gc.pre[1];
-    xr4 = gc.pre[3];
-    qr4 = gc.pre[4];
-  } else {
-    xi4 = s.x[hdr.y];
-    qi4 = s.q[hdr.y];
-    xr4 = s.x[hdr.z];
-    qr4 = s.q[hdr.z];
-  }
+XD void velocity_floor8(const Dev6& s, int i, const Par6& p, const Grp& G) {
+  // every load first (one round trip), then the arithmetic
+  const float4 x4 = s.x[i], q4i = s.q[i], I4 = s.inv_I[i], he4 = s.he[i], v4 = s.v[i], w4 = s.w[i];
   const int c = G.l;
-  return box_pair8_core(s, pid, G, hdr, gc.nrm, gc.off_inc[c], gc.off_ref[c], gc.lam[c], xi4, qi4, gc.pre[2], xr4,
-                        qr4, gc.pre[5], &gc.lam[c]);
-}
-
-// kernels_6dof.py:542-590 on eight lanes, from the body's records and the
-// lane's corner multiplier.
-XD void velocity_floor8_core(const Dev6& s, int i, const Par6& p, const Grp& G, float4 x4, float4 q4i, float4 I4,
-                             float4 he4, float4 v4, float4 w4, float lam_n) {
-  const int c = G.l;
+  const float lam_n = s.lam_floor[8 * i + c];
   float im = x4.w;
   if (im == 0.0f) return;
   const V3 S = V3{0.0f, 1.0f, 0.0f};
@@ -959,32 +876,22 @@ XD void velocity_floor8_core(const Dev6& s, int i, const Par6& p, const Grp& G, 
   }
 }
 
-XD void velocity_floor8(const Dev6& s, int i, const Par6& p, const Grp& G) {
-  // every load first (one round trip), then the arithmetic
-  const float4 x4 = s.x[i], q4i = s.q[i], I4 = s.inv_I[i], he4 = s.he[i], v4 = s.v[i], w4 = s.w[i];
-  const float lam_n = s.lam_floor[8 * i + G.l];
-  velocity_floor8_core(s, i, p, G, x4, q4i, I4, he4, v4, w4, lam_n);
-}
-
-// The group's cached floor body: extents, inertia and the corner's multiplier
-// from shared memory, the finalized pose and velocities from memory.
-XD void velocity_floor8_cached(const Dev6& s, int i, const Par6& p, const Grp& G, const GroupCache& gc) {
-  const float4 x4 = s.x[i], q4i = s.q[i], v4 = s.v[i], w4 = s.w[i];
-  velocity_floor8_core(s, i, p, G, x4, q4i, gc.pre[3], gc.pre[2], v4, w4, gc.lam[G.l]);
-}
-
-// kernels_6dof.py:594-659 on eight lanes, from the pair's records.
-XD void velocity_box8_core(const Dev6& s, int pid, const Par6& p, const Grp& G, int4 hdr, float4 nrm, float4 off_i,
-                           float4 off_j, float lam_slot, float4 xi4, float4 qi4, float4 Ii4, float4 vi4, float4 wi4,
-                           float4 xj4, float4 qj4, float4 Ij4, float4 vj4, float4 wj4) {
+XD void velocity_box8(const Dev6& s, int pid, const Par6& p, const Grp& G) {
+  // the pair's own records with the header (one round trip), the bodies next
   const int c = G.l;
+  const int slot = 8 * pid + c;
+  int4 hdr = s.m_hdr[pid];
+  const float4 nrm = s.m_normal[pid], off_i = s.m_off_inc[slot], off_j = s.m_off_ref[slot];
+  const float lam_slot = s.lam_pair[slot];
   const int nc = hdr.x;
+  if (nc == 0) return;
   const int ci = hdr.y, cj = hdr.z;
   V3 S = v3(nrm);
+  float4 xi4 = s.x[ci], xj4 = s.x[cj];
   V3 xi = v3(xi4), xj = v3(xj4);
-  Q4 qi = q4(qi4), qj = q4(qj4);
-  V3 Ii = v3(Ii4), Ij = v3(Ij4);
-  V3 vi = v3(vi4), vj = v3(vj4), wi = v3(wi4), wj = v3(wj4);
+  Q4 qi = q4(s.q[ci]), qj = q4(s.q[cj]);
+  V3 Ii = v3(s.inv_I[ci]), Ij = v3(s.inv_I[cj]);
+  V3 vi = v3(s.v[ci]), vj = v3(s.v[cj]), wi = v3(s.w[ci]), wj = v3(s.w[cj]);
   const float imi = xi4.w, imj = xj4.w;
   V3 dvi = V3{0, 0, 0}, dwi = V3{0, 0, 0}, dvj = V3{0, 0, 0}, dwj = V3{0, 0, 0};
   float ni = 0.0f, nj = 0.0f;
@@ -1036,61 +943,10 @@ XD void velocity_box8_core(const Dev6& s, int pid, const Par6& p, const Grp& G, 
   }
 }
 
-XD void velocity_box8(const Dev6& s, int pid, const Par6& p, const Grp& G) {
-  // the pair's own records with the header (one round trip), the bodies next
-  const int slot = 8 * pid + G.l;
-  int4 hdr = s.m_hdr[pid];
-  const float4 nrm = s.m_normal[pid], off_i = s.m_off_inc[slot], off_j = s.m_off_ref[slot];
-  const float lam_slot = s.lam_pair[slot];
-  if (hdr.x == 0) return;
-  const int ci = hdr.y, cj = hdr.z;
-  velocity_box8_core(s, pid, p, G, hdr, nrm, off_i, off_j, lam_slot, s.x[ci], s.q[ci], s.inv_I[ci], s.v[ci], s.w[ci],
-                     s.x[cj], s.q[cj], s.inv_I[cj], s.v[cj], s.w[cj]);
-}
-
-// The group's cached pair: manifold, multipliers and inertias from shared
-// memory, the finalized poses and velocities from memory.
-XD void velocity_box8_cached(const Dev6& s, int pid, const Par6& p, const Grp& G, const GroupCache& gc) {
-  const int4 hdr = gc.hdr;
-  if (hdr.x == 0) return;
-  const int ci = hdr.y, cj = hdr.z, c = G.l;
-  velocity_box8_core(s, pid, p, G, hdr, gc.nrm, gc.off_inc[c], gc.off_ref[c], gc.lam[c], s.x[ci], s.q[ci],
-                     gc.pre[2], s.v[ci], s.w[ci], s.x[cj], s.q[cj], gc.pre[5], s.v[cj], s.w[cj]);
-}
-
-// Prefetch of the group's cached pair's bodies (x, q, inv_I of the incident,
-// then of the reference body) into shared memory for the next phase.
-XD void prefetch_pair8(const Dev6& s, GroupCache& gc, const Grp& G) {
-  const int4 h = gc.hdr;
-  if (h.x == 0 || G.l >= 6) return;
-  const int b = G.l < 3 ? h.y : h.z, k = G.l % 3;
-  cp_async16(&gc.pre[G.l], k == 0 ? s.x + b : (k == 1 ? s.q + b : s.inv_I + b));
-}
-
-// Prefetch of the group's cached floor body (x, q, he, inv_I, x_prev, q_prev).
-XD void prefetch_floor8(const Dev6& s, int i, GroupCache& gc, const Grp& G) {
-  if (G.l >= 6) return;
-  const float4* src[6] = {s.x + i, s.q + i, s.he + i, s.inv_I + i, s.xp + i, s.qp + i};
-  cp_async16(&gc.pre[G.l], src[G.l]);
-}
-
 // generate_box_manifold with 8 lanes; `stage` is this group's 8-vertex buffer.
-// gc (shared memory, or null): also record the manifold and the zeroed
-// multipliers in the group's cache; ab_cached: take the pair's bodies from it.
-XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float4* stage, int edge_axes = 0,
-                       GroupCache* gc = nullptr, bool ab_cached = false) {
+XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float4* stage, int edge_axes = 0) {
   s.lam_pair[8 * pid + G.l] = 0.0f;
-  int2 pr;
-  if (ab_cached) {
-    pr = gc->ab;
-  } else {
-    pr = s.pairs[pid];
-    if (gc && G.l == 0) gc->ab = pr;
-  }
-  if (gc) {
-    gc->lam[G.l] = 0.0f;
-    if (G.l == 0) gc->hdr = make_int4(0, 0, 0, 0);  // a pair whose manifold is empty
-  }
+  int2 pr = s.pairs[pid];
   const int a = pr.x, b = pr.y;
   V3 cA = v3(s.x[a]), cB = v3(s.x[b]), eA = v3(s.he[a]), eB = v3(s.he[b]);
   M33 RA = q2m(q4(s.q[a])), RB = q2m(q4(s.q[b]));
@@ -1211,21 +1067,12 @@ XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float
   int rank = gscan_ex(G, keep ? 1 : 0, &nc);
   if (keep) {
     V3 p_ref = v - ref_face_n * d_signed;
-    const float4 oi = f4(mtv(R_inc, v - c_inc), 0.0f), orf = f4(mtv(R_ref, p_ref - c_ref), 0.0f);
-    s.m_off_inc[8 * pid + rank] = oi;
-    s.m_off_ref[8 * pid + rank] = orf;
-    if (gc) {
-      gc->off_inc[rank] = oi;
-      gc->off_ref[rank] = orf;
-    }
+    s.m_off_inc[8 * pid + rank] = f4(mtv(R_inc, v - c_inc), 0.0f);
+    s.m_off_ref[8 * pid + rank] = f4(mtv(R_ref, p_ref - c_ref), 0.0f);
   }
   if (G.l == 0) {
     s.m_hdr[pid] = make_int4(nc, inc_b, ref_b, 0);
     s.m_normal[pid] = f4(ref_face_n, 0.0f);
-    if (gc) {
-      gc->hdr = make_int4(nc, inc_b, ref_b, 0);
-      gc->nrm = f4(ref_face_n, 0.0f);
-    }
   }
 }
 
@@ -1282,21 +1129,8 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
 
 // Persistent substep kernel, quarter-warp phases (manifold, floor, box,
 // velocity): same phase order and barriers as k6_substeps.
-//
-// Items of the contact phases are laid out pairs first (group g: pair g, then
-// floor body g - np), so a lane group meets the same first pair, or the same
-// first floor body, in every phase of a substep.  That item's records live in
-// the group's shared-memory cache (GroupCache): the manifold the group
-// generated and each lane's multiplier, so the solve and velocity phases
-// fetch only the bodies' changing state; and the bodies of the first
-// iteration are prefetched with cp.async at the end of the manifold phase,
-// where no phase writes them, so they arrive during the barrier and the first
-// iteration starts with every input on chip.  Further items of a group (scenes
-// with more items than lane groups) and the edge-axis manifold take the
-// memory path.  The arithmetic is the same functions' either way.
 __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier bar) {
   __shared__ float4 stage[512 / 8][8];
-  __shared__ GroupCache gcache[512 / 8];
   const int n = s.n, nj = s.nj;
   const int np = min(*s.n_pairs, s.cap);
   unsigned pts = 0;  // manifold points of this thread's pairs, every substep
@@ -1304,10 +1138,6 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
   const Grp G = grp8();
   const int g0 = t0 >> 3, gs = st >> 3;
   float4* my_stage = stage[threadIdx.x >> 3];
-  GroupCache& gc = gcache[threadIdx.x >> 3];
-  const bool use_cache = p.edge_axes == 0;
-  const bool own_pair = use_cache && g0 < np;                    // the group's first pair: g0
-  const bool own_floor = use_cache && g0 >= np && g0 - np < n;   // the group's first floor body: g0 - np
   const int nb = max(n, nj);
   for (int i = t0; i < nb; i += st) {
     if (i < n) body_integrate6(s, i, p);
@@ -1316,28 +1146,15 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
   grid_sync(bar);
   for (int sub = 0; sub < p.substeps; ++sub) {
     const bool more = sub + 1 < p.substeps;
-    for (int pid = g0; pid < np; pid += gs) {
-      const bool cached = own_pair && pid == g0;
-      manifold_pair8(s, pid, p.margin, G, my_stage, p.edge_axes, cached ? &gc : nullptr, cached && sub > 0);
-    }
-    if (own_pair) {
-      __syncwarp(G.mask);  // the header lane 0 recorded
-      prefetch_pair8(s, gc, G);
-    } else if (own_floor) {
-      gc.lam[G.l] = 0.0f;  // the substep's integrate zeroed the corners' multipliers
-      prefetch_floor8(s, g0 - np, gc, G);
-    }
+    for (int pid = g0; pid < np; pid += gs) manifold_pair8(s, pid, p.margin, G, my_stage, p.edge_axes);
     grid_sync(bar);
     for (int it = 0; it < p.iterations; ++it) {
       for (int t = t0; t < nj; t += st) joint_row(s, t, p.h);
       for (int g = g0; g < n + np; g += gs) {
-        if (g < np) {
-          const int nc = (own_pair && g == g0) ? box_pair8_cached(s, g, G, gc, it == 0) : box_pair8(s, g, G);
+        if (g < n) floor_body8(s, g, p, G);
+        else {
+          const int nc = box_pair8(s, g - n, G);
           if (it == 0 && G.l == 0) pts += nc;
-        } else if (own_floor && g == g0) {
-          floor_body8_cached(s, g - np, p, G, gc, it == 0);
-        } else {
-          floor_body8(s, g - np, p, G);
         }
       }
       grid_sync(bar);
@@ -1346,22 +1163,12 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
       grid_sync(bar);
     }
     if (p.iterations == 0) {
-      if (own_pair || own_floor) {  // the prefetch is not consumed by a solve
-        cp_async_wait_all();
-        __syncwarp(G.mask);
-      }
       for (int i = t0; i < n; i += st) body_finalize6(s, i, p);
       grid_sync(bar);
     }
     for (int g = g0; g < n + np; g += gs) {
-      if (g < np) {
-        if (own_pair && g == g0) velocity_box8_cached(s, g, p, G, gc);
-        else velocity_box8(s, g, p, G);
-      } else if (own_floor && g == g0) {
-        velocity_floor8_cached(s, g - np, p, G, gc);
-      } else {
-        velocity_floor8(s, g - np, p, G);
-      }
+      if (g < n) velocity_floor8(s, g, p, G);
+      else velocity_box8(s, g - n, p, G);
     }
     grid_sync(bar);
     for (int i = t0; i < nb; i += st) {
