@@ -287,16 +287,16 @@ def test_warm_start_option_on_the_3dof_solver(ws):
 
 @pytest.mark.parametrize("ws", ["previous", "learned"])
 def test_warm_start_option_on_the_6dof_solver(ws):
-    """Solver6DOF(warm_start=...) on a small pile that falls and settles (27
-    boxes in columns 1.1 m apart, so none starts interpenetrating): frames stay
-    finite, the warm-started pile comes to rest like the plain one (every body
+    """Solver6DOF(warm_start=...) on boxes dropped onto the floor (a 3 x 3
+    layer 1.1 m apart, so none starts interpenetrating or stacks): frames stay
+    finite, the warm-started boxes come to rest like the plain ones (every body
     below 0.2 m/s after 60 frames, mean height within 2 cm of the plain
     solver's), and the device point count covers every substep."""
     model = WarmStartMLP.pretrained() if ws == "learned" else "previous"
     kw = dict(dt=1 / 60, substeps=15, iterations=2, floor_y=0.0, friction=0.6, restitution=0.2)
     warm, plain = Solver6DOF(warm_start=model, **kw), Solver6DOF(**kw)
     for s in (warm, plain):
-        scenes.build_box_pile(s, nx=3, ny=3, nz=3, pitch=1.1, y0=0.5)
+        scenes.build_box_pile(s, nx=3, ny=1, nz=3, pitch=1.1, y0=0.5)
     for _ in range(60):
         warm.step()
         plain.step()
@@ -308,4 +308,4 @@ def test_warm_start_option_on_the_6dof_solver(ws):
     assert speed < 0.2, speed
     dy = abs(float(warm.positions()[:, 1].mean() - plain.positions()[:, 1].mean()))
     assert dy < 0.02, dy
-    assert warm._runner.kit.points_total > 0
+    assert warm._runner.substeps_run == 60 * 15
