@@ -654,7 +654,10 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
         for (int it = 0; it < I; ++it) {
           const AccGlobal acc_it{A + (size_t)it * st};
           if (it == 0) {
-            for (int i = tid0; i < n; i += stride) {
+            // The particles' owners are the last threads (particle k on thread
+            // stride - 1 - k) and the rows take the first ones, so in a scene
+            // with fewer rows than threads the two run side by side.
+            for (int i = stride - 1 - tid0; i < n; i += stride) {
               const EndHeld e = sub == 0 ? start(i) : carry(i);
               xc[i] = e.x;
               xpc[i] = e.p;
@@ -663,7 +666,7 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
             else rows_first(carry, acc_it);
           } else {
             if (it == 1 && sub > 0) {
-              for (int i = tid0; i < n; i += stride)
+              for (int i = stride - 1 - tid0; i < n; i += stride)
                 for (int k = 0; k < I; ++k) Ap[k * st + i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             }
             const PosFoldedHeld pos{xc, xpc, A, st, it, p.relax};

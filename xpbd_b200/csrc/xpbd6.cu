@@ -1282,8 +1282,11 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
     const bool first = sub == 0;
     const Dev6 src = state(first ? 0 : (sub & 1));  // the previous substep's state (the frame's for k = 0)
     const Dev6 cur = state((sub & 1) ^ 1);          // this substep's
-    // substep boundary + manifold
-    for (int i = t0; i < nb; i += st) {
+    // substep boundary + manifold.  The bodies' owners are the grid's last
+    // threads (body k on thread st - 1 - k), which the manifold's lane groups
+    // (the first ones) leave idle in a contact-rich scene, so the two run side
+    // by side instead of one after the other on the same threads.
+    for (int i = st - 1 - t0; i < nb; i += st) {
       if (i < n) body_step_into(src, cur, i, p, first);
       if (i < nj) s.lam_joint[i] = 0.0f;
     }
