@@ -51,9 +51,8 @@ def test_phase_counts_of_the_frame_kernels():
     b = Solver6DOF(device="cuda:0", dt=1 / 60, substeps=15, iterations=2)
     scenes.build_box_pile(b, nx=3, ny=2, nz=3)
     b.step()
-    # eight lanes: the substep boundary folded into the manifold phase, 6 barriers
-    # per substep and a closing pass; one lane: the integrate pass + 7 per substep
-    assert b.phases() == (15 * 6, 15 * 6 + 1)
+    # the integrate pass + 7 per substep, for both lane widths
+    assert b.phases() == (1 + 15 * 7,) * 2
     b.lanes = 1
     b.step()
     assert b.phases() == (1 + 15 * 7,) * 2

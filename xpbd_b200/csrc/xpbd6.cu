@@ -38,9 +38,6 @@ struct Dev6 {
   const float4* j_b;  // anchor in B's frame, compliance in w
   float* lam_joint;
   const int* scene;  // per body (NULL: one scene)
-  // second x, q, v, w buffers (handle memory): the eight-lane substep kernel
-  // alternates the substeps' states between these and x, q, v, w
-  float4 *x1 = nullptr, *q1 = nullptr, *v1 = nullptr, *w1 = nullptr;
   // manifold points summed over the substeps of every frame run (NULL: not
   // counted); the benchmark's projection count
   unsigned long long* points;
@@ -664,97 +661,6 @@ XD void body_velocity_integrate6(const Dev6& s, int i, const Par6& p, bool more)
   s.q[i] = f4(quat_integrate(q, wi, p.h));
 }
 
-// A body's state at the start of the next substep, computed from the state
-// `src` holds after the velocity solve (its averaged velocity corrections still
-// in av / aw): the velocity apply and clamp, then the integrate -- the same
-// expressions, in the same order, as body_velocity_integrate6 with `more`.
-// first: the frame's first substep, a plain integrate (body_integrate6: no
-// pending corrections and no clamp).  Pure: the body's owner stores the result,
-// and the manifold lanes of the same phase recompute it for their two bodies.
-struct Stepped {
-  float4 x, q, v, w;
-};
-XD Stepped stepped_state(const Dev6& src, int i, const Par6& p, bool first) {
-  const float4 x4 = src.x[i], qv = src.q[i], v4 = src.v[i], w4 = src.w[i];
-  const float4 I4 = p.gyro ? src.inv_I[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  V3 vi = v3(v4), wi = v3(w4);
-  if (!first) {
-    const float4 a = src.av[i], aw4 = src.aw[i];
-    const int n = (int)a.w;
-    if (n > 0 && x4.w > 0.0f) {
-      float inv_n = 1.0f / (float)n;
-      vi = vi + v3(a) * inv_n;
-      wi = wi + v3(aw4) * inv_n;
-    }
-    if (p.max_speed > 0.0f) {
-      float sp = length(vi);
-      if (sp > p.max_speed) vi = vi * (p.max_speed / sp);
-      float sa = length(wi);
-      if (p.max_omega > 0.0f && sa > p.max_omega) wi = wi * (p.max_omega / sa);
-    }
-  }
-  if (x4.w == 0.0f) return Stepped{x4, qv, f4(vi, 0.0f), f4(wi, 0.0f)};
-  vi = vi + V3{p.gx, p.gy, p.gz} * p.h;
-  const float4 xn = f4(v3(x4) + vi * p.h, x4.w);
-  Q4 q = q4(qv);
-  if (p.gyro) {
-    V3 wb = qrot_inv(q, wi);
-    V3 ii = v3(I4);
-    float ix = ii.x > 0.0f ? 1.0f / ii.x : 0.0f;
-    float iy = ii.y > 0.0f ? 1.0f / ii.y : 0.0f;
-    float iz = ii.z > 0.0f ? 1.0f / ii.z : 0.0f;
-    V3 Iw = V3{ix * wb.x, iy * wb.y, iz * wb.z};
-    V3 tau = -cross(wb, Iw);
-    V3 dwb = V3{ii.x * tau.x, ii.y * tau.y, ii.z * tau.z} * p.h;
-    wi = wi + qrot(q, dwb);
-  }
-  return Stepped{xn, f4(quat_integrate(q, wi, p.h)), f4(vi, 0.0f), f4(wi, 0.0f)};
-}
-
-// The owner's part of the folded substep boundary: store body i's stepped
-// state into dst and record the substep start (x_prev, q_prev, zeroed floor
-// multipliers).  The velocity accumulators are cleared later, once the
-// manifold lanes that read them are done.
-XD void body_step_into(const Dev6& src, const Dev6& dst, int i, const Par6& p, bool first) {
-  const Stepped st = stepped_state(src, i, p, first);
-  dst.xp[i] = src.x[i];
-  dst.qp[i] = src.q[i];
-#pragma unroll
-  for (int c = 0; c < 8; ++c) dst.lam_floor[8 * i + c] = 0.0f;
-  dst.x[i] = st.x;
-  dst.q[i] = st.q;
-  dst.v[i] = st.v;
-  dst.w[i] = st.w;
-}
-
-// The frame's closing pass: the last substep's velocity apply and clamp
-// (body_velocity_integrate6 without `more`), read from `cur` and stored, with
-// the pose, into the frame state `out`.
-XD void body_velocity_final6(const Dev6& cur, const Dev6& out, int i, const Par6& p) {
-  const float4 a = cur.av[i], aw4 = cur.aw[i], v4 = cur.v[i], w4 = cur.w[i], x4 = cur.x[i], qv = cur.q[i];
-  int n = (int)a.w;
-  V3 vi = v3(v4), wi = v3(w4);
-  if (n > 0 && x4.w > 0.0f) {
-    float inv_n = 1.0f / (float)n;
-    vi = vi + v3(a) * inv_n;
-    wi = wi + v3(aw4) * inv_n;
-  }
-  cur.av[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  cur.aw[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  if (p.max_speed > 0.0f) {
-    float sp = length(vi);
-    if (sp > p.max_speed) vi = vi * (p.max_speed / sp);
-    float sa = length(wi);
-    if (p.max_omega > 0.0f && sa > p.max_omega) wi = wi * (p.max_omega / sa);
-  }
-  out.v[i] = f4(vi, 0.0f);
-  out.w[i] = f4(wi, 0.0f);
-  if (out.x != cur.x) {
-    out.x[i] = x4;
-    out.q[i] = qv;
-  }
-}
-
 // =================================================================================
 // Quarter-warp variants: 8 lanes cooperate on one floor body (one lane per box
 // corner), one contact pair (one lane per manifold point) or one manifold
@@ -1038,30 +944,12 @@ XD void velocity_box8(const Dev6& s, int pid, const Par6& p, const Grp& G) {
 }
 
 // generate_box_manifold with 8 lanes; `stage` is this group's 8-vertex buffer.
-// STEPPED: the bodies' poses are the substep-start poses stepped from src's
-// state in this same phase (stepped_state, the folded substep boundary of
-// k6_substeps8) instead of s's stored poses.
-template <bool STEPPED>
-XD void manifold_pair8_t(const Dev6& s, const Dev6& src, const Par6& sp, bool first, int pid, float margin,
-                         const Grp& G, float4* stage, int edge_axes) {
+XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float4* stage, int edge_axes = 0) {
   s.lam_pair[8 * pid + G.l] = 0.0f;
   int2 pr = s.pairs[pid];
   const int a = pr.x, b = pr.y;
-  V3 cA, cB;
-  M33 RA, RB;
-  if (STEPPED) {
-    const Stepped sa = stepped_state(src, a, sp, first), sb = stepped_state(src, b, sp, first);
-    cA = v3(sa.x);
-    cB = v3(sb.x);
-    RA = q2m(q4(sa.q));
-    RB = q2m(q4(sb.q));
-  } else {
-    cA = v3(s.x[a]);
-    cB = v3(s.x[b]);
-    RA = q2m(q4(s.q[a]));
-    RB = q2m(q4(s.q[b]));
-  }
-  const V3 eA = v3(s.he[a]), eB = v3(s.he[b]);
+  V3 cA = v3(s.x[a]), cB = v3(s.x[b]), eA = v3(s.he[a]), eB = v3(s.he[b]);
+  M33 RA = q2m(q4(s.q[a])), RB = q2m(q4(s.q[b]));
   V3 cBA = cA - cB;
   // SAT: lane l < 3 tests A's axis l, lane 3..5 tests B's axis l-3
   float ov = INFINITY;
@@ -1188,10 +1076,6 @@ XD void manifold_pair8_t(const Dev6& s, const Dev6& src, const Par6& sp, bool fi
   }
 }
 
-XD void manifold_pair8(const Dev6& s, int pid, float margin, const Grp& G, float4* stage, int edge_axes = 0) {
-  manifold_pair8_t<false>(s, s, Par6{}, false, pid, margin, G, stage, edge_axes);
-}
-
 // ---------------------------------------------------------------------------------
 // Persistent substep kernel: every substep of one frame in one launch.
 __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier bar) {
@@ -1244,19 +1128,7 @@ __global__ void __launch_bounds__(512) k6_substeps(Dev6 s, Par6 p, GridBarrier b
 }
 
 // Persistent substep kernel, quarter-warp phases (manifold, floor, box,
-// velocity): the phases of k6_substeps with the substep boundary folded.
-//
-// The velocity apply + integrate that opens a substep runs in the same phase
-// as its manifold: each body's owner stores the stepped state (stepped_state)
-// in the other of two state buffers (x, q, v, w and x1, q1, v1, w1; substep k
-// reads buffer k & 1 ... the frame state for k = 0, and writes the other),
-// while the manifold lanes recompute the stepped poses of their two bodies
-// from the buffer being read.  Same expressions, same order, so the values are
-// bit-identical to the unfolded phases; a substep has 2I + 2 barriers instead
-// of 2I + 3, and the frame drops its separate first integrate.  The velocity
-// accumulators the stepped state reads are cleared in the first solve phase.
-// A closing pass applies the last substep's velocities and stores the frame
-// state in x, q, v, w.
+// velocity): same phase order and barriers as k6_substeps.
 __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier bar) {
   __shared__ float4 stage[512 / 8][8];
   const int n = s.n, nj = s.nj;
@@ -1267,69 +1139,43 @@ __global__ void __launch_bounds__(512) k6_substeps8(Dev6 s, Par6 p, GridBarrier 
   const int g0 = t0 >> 3, gs = st >> 3;
   float4* my_stage = stage[threadIdx.x >> 3];
   const int nb = max(n, nj);
-  // state buffer b: 0 = x, q, v, w; 1 = x1, q1, v1, w1
-  auto state = [&](int b) {
-    Dev6 d = s;
-    if (b) {
-      d.x = s.x1;
-      d.q = s.q1;
-      d.v = s.v1;
-      d.w = s.w1;
-    }
-    return d;
-  };
+  for (int i = t0; i < nb; i += st) {
+    if (i < n) body_integrate6(s, i, p);
+    if (i < nj) s.lam_joint[i] = 0.0f;
+  }
+  grid_sync(bar);
   for (int sub = 0; sub < p.substeps; ++sub) {
-    const bool first = sub == 0;
-    const Dev6 src = state(first ? 0 : (sub & 1));  // the previous substep's state (the frame's for k = 0)
-    const Dev6 cur = state((sub & 1) ^ 1);          // this substep's
-    // substep boundary + manifold.  The bodies' owners are the grid's last
-    // threads (body k on thread st - 1 - k), which the manifold's lane groups
-    // (the first ones) leave idle in a contact-rich scene, so the two run side
-    // by side instead of one after the other on the same threads.
-    for (int i = st - 1 - t0; i < nb; i += st) {
-      if (i < n) body_step_into(src, cur, i, p, first);
-      if (i < nj) s.lam_joint[i] = 0.0f;
-    }
-    for (int pid = g0; pid < np; pid += gs)
-      manifold_pair8_t<true>(cur, src, p, first, pid, p.margin, G, my_stage, p.edge_axes);
+    const bool more = sub + 1 < p.substeps;
+    for (int pid = g0; pid < np; pid += gs) manifold_pair8(s, pid, p.margin, G, my_stage, p.edge_axes);
     grid_sync(bar);
     for (int it = 0; it < p.iterations; ++it) {
-      if (it == 0) {  // the accumulators the stepped state read
-        for (int i = t0; i < n; i += st) {
-          s.av[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-          s.aw[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-      }
-      for (int t = t0; t < nj; t += st) joint_row(cur, t, p.h);
+      for (int t = t0; t < nj; t += st) joint_row(s, t, p.h);
       for (int g = g0; g < n + np; g += gs) {
-        if (g < n) floor_body8(cur, g, p, G);
+        if (g < n) floor_body8(s, g, p, G);
         else {
-          const int nc = box_pair8(cur, g - n, G);
+          const int nc = box_pair8(s, g - n, G);
           if (it == 0 && G.l == 0) pts += nc;
         }
       }
       grid_sync(bar);
       const bool last = it + 1 == p.iterations;
-      for (int i = t0; i < n; i += st) body_apply_finalize6(cur, i, p, last);
+      for (int i = t0; i < n; i += st) body_apply_finalize6(s, i, p, last);
       grid_sync(bar);
     }
     if (p.iterations == 0) {
-      for (int i = t0; i < n; i += st) {
-        s.av[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        s.aw[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        body_finalize6(cur, i, p);
-      }
+      for (int i = t0; i < n; i += st) body_finalize6(s, i, p);
       grid_sync(bar);
     }
     for (int g = g0; g < n + np; g += gs) {
-      if (g < n) velocity_floor8(cur, g, p, G);
-      else velocity_box8(cur, g - n, p, G);
+      if (g < n) velocity_floor8(s, g, p, G);
+      else velocity_box8(s, g - n, p, G);
     }
     grid_sync(bar);
-  }
-  if (p.substeps > 0) {  // the last substep's velocity apply; the frame state back in x, q, v, w
-    const Dev6 cur = state(((p.substeps - 1) & 1) ^ 1);
-    for (int i = t0; i < n; i += st) body_velocity_final6(cur, s, i, p);
+    for (int i = t0; i < nb; i += st) {
+      if (i < n) body_velocity_integrate6(s, i, p, more);
+      if (more && i < nj) s.lam_joint[i] = 0.0f;
+    }
+    grid_sync(bar);
   }
   add_points(s.points, pts);
   grid_exit(bar);
@@ -2629,8 +2475,7 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
          o_fl = take(4 * (size_t)n), o_cnt = take(4 * 14 * (size_t)n), o_off = take(4 * 14 * (size_t)n),
          o_sc = take(scan_scratch_bytes(14 * n)), o_cell = take(16 * (size_t)n), o_ck = take(8 * (size_t)n),
          o_cv = take(4 * (size_t)n), o_red = take(64), o_half = take(16 * (size_t)n),
-         o_roots = take(4 * (size_t)std::max(s->scene ? s->n_scenes : 1, 1)),
-         o_state1 = take(4 * 16 * (size_t)n);  // the eight-lane kernel's second x, q, v, w buffers
+         o_roots = take(4 * (size_t)std::max(s->scene ? s->n_scenes : 1, 1));
   if (off > h->buf_bytes) {
     if (h->buf) cudaFree(h->buf);
     h->buf = nullptr;
@@ -2659,11 +2504,6 @@ extern "C" int xpbd6_bind(xpbd6_solver* h, const xpbd6_state* s, const xpbd6_par
   q.red = reinterpret_cast<int*>(b + o_red);
   q.half = reinterpret_cast<float4*>(b + o_half);
   q.roots = reinterpret_cast<int*>(b + o_roots);
-  float4* s1 = reinterpret_cast<float4*>(b + o_state1);
-  h->dev.x1 = s1;
-  h->dev.q1 = s1 + n;
-  h->dev.v1 = s1 + 2 * (size_t)n;
-  h->dev.w1 = s1 + 3 * (size_t)n;
   long long work = std::max<long long>((long long)s->n_bodies + s->n_joints, s->pair_capacity / 2);
   int mode = h->force_mode;
   // automatic: one cluster for small scenes (its barrier is the cheapest); the
@@ -2888,27 +2728,16 @@ extern "C" int xpbd6_morton(xpbd6_solver* h, unsigned* codes_out, void* stream) 
   return XPBD_OK;
 }
 
-// Barriers and phases of one frame of the bound substep kernel.  k6_substeps:
-// the integrate pass, then per substep the manifold, (solve, apply) per
-// iteration (a finalize pass when there are none), the velocity solve and the
-// velocity apply + integrate, each closed by a barrier.  k6_substeps8 folds the
-// velocity apply + integrate into the next manifold phase: per substep the
-// stepped state + manifold, (solve, apply) per iteration, the velocity solve,
-// each closed by a barrier, and a closing pass without one.
+// Barriers and phases of one frame of k6_substeps / k6_substeps8 as bound: the
+// integrate pass, then per substep the manifold, (solve, apply) per iteration
+// (a finalize pass when there are none), the velocity solve and the velocity
+// apply + integrate, each closed by a barrier.
 extern "C" int xpbd6_phases(xpbd6_solver* h, int* barriers, int* phases) {
   if (!h) return XPBD_ERR_BAD_ARG;
   const int S = h->par.substeps, I = h->par.iterations;
-  const long long per = I > 0 ? 2 * I : 1;
-  long long b, ph;
-  if (h->lanes == 8) {
-    b = (long long)S * (1 + per + 1);
-    ph = b + (S > 0 ? 1 : 0);
-  } else {
-    b = 1 + (long long)S * (1 + per + 2);
-    ph = b;
-  }
+  const long long b = 1 + (long long)S * (1 + (I > 0 ? 2 * I : 1) + 2);
   if (barriers) *barriers = (int)b;
-  if (phases) *phases = (int)ph;
+  if (phases) *phases = (int)b;
   return XPBD_OK;
 }
 
