@@ -217,9 +217,16 @@ int xpbd_mlp_num_params(void);
  * weff = w + alpha~ (0 = row not warm-started). */
 int xpbd3_features(const xpbd3_state* s, float h, float gx, float gy, float gz, float* feats, float* weff,
                    void* stream);
-/* lambda0[j] = slog^-1(MLP(feats[j])) 1 mm / weff[j] for m rows (bf16 weights). */
+/* lambda0[j] = slog^-1(MLP(feats[j])) 1 mm / weff[j] for m rows (bf16 weights).
+ * The 64 x 64 layer runs on the tensor cores (tcgen05, 128-row tiles, bf16
+ * operands, fp32 accumulator in tensor memory); the first layer's activations
+ * are rounded to bf16.  feats: m x 8 floats (7 used). */
 int xpbd_mlp_infer(const float* feats, const float* weff, int m, const void* weights_bf16, float* lam0,
                    void* stream);
+/* 1 in *status if an inference launch gave up waiting for the tensor core
+ * (bounded wait; that launch wrote its remaining rows as NaN), else 0;
+ * reset != 0 clears it.  Synchronous. */
+int xpbd_mlp_status(int* status, int reset);
 /* Loss (mean squared error) of a batch and its gradient, added into G. */
 int xpbd_mlp_grads(const float* feats, const float* targets, int B, const void* weights_bf16, float* G,
                    float* loss, void* stream);

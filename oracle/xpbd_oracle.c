@@ -1322,6 +1322,14 @@ float or_bf16_round(float x) {
 }
 
 static float or_gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+
+/* The first layer's activations are rounded to bf16, as the engine does for
+ * the operand of its tensor-core second layer (the gradient passes straight
+ * through the rounding).  or_mlp_round_activations(0) turns the rounding off,
+ * so that finite differences of the loss can check the gradient formulas. */
+static int or_mlp_act_bf16 = 1;
+void or_mlp_round_activations(int on) { or_mlp_act_bf16 = on; }
+static float or_act(float a) { return or_mlp_act_bf16 ? or_bf16_round(a) : a; }
 static float or_gelu_d(float x) {
     return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
 }
@@ -1343,7 +1351,7 @@ double or_mlp_grads(const float *feats, const float *targets, int B, const float
         for (int u = 0; u < MLP_H; ++u) {
             float z = B1[u];
             for (int k = 0; k < MLP_IN; ++k) z = fmaf(W1[u * MLP_IN + k], x[k], z);
-            z1[u] = z; a1[u] = or_gelu(z);
+            z1[u] = z; a1[u] = or_act(or_gelu(z));
         }
         for (int u = 0; u < MLP_H; ++u) {
             float z = B2[u];
@@ -1391,7 +1399,7 @@ void or_mlp_forward(const float *feats, int B, const float *w_in, float *y_out) 
         for (int u = 0; u < MLP_H; ++u) {
             float z = B1[u];
             for (int k = 0; k < MLP_IN; ++k) z = fmaf(W1[u * MLP_IN + k], x[k], z);
-            a1[u] = or_gelu(z);
+            a1[u] = or_act(or_gelu(z));
         }
         float y = B3[0];
         for (int u = 0; u < MLP_H; ++u) {

@@ -58,7 +58,46 @@ def test_mlp_inference_matches_oracle():
     y = np.zeros(m_rows, np.float32)
     O.lib().or_mlp_forward(O.fp(np.ascontiguousarray(feats)), m_rows, O.fp(m.w.cpu().numpy()), O.fp(y))
     ref = np.sign(y) * np.expm1(np.abs(y)) * 1e-3 / weff
-    np.testing.assert_allclose(lam0.cpu().numpy(), ref, rtol=1e-4, atol=1e-9)
+    got = lam0.cpu().numpy()
+    assert np.isfinite(got).all()
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-9)
+    # The second layer runs on the tensor cores (bf16 operands, fp32
+    # accumulation in an order of its own).  Both sides round the first layer's
+    # GELU outputs to bf16; a GELU result (CUDA erff against the host's) within
+    # an ulp of a rounding boundary can round to the neighbouring bf16 value
+    # (0.4 % of that activation), so a few rows move by up to ~1e-3; the rest
+    # agree to the fp32 accumulation.
+    assert rel.max() <= 2e-3, rel.max()
+    assert np.mean(rel <= 2e-5) >= 0.95, np.quantile(rel, [0.5, 0.95, 0.99])
+    st = C.c_int(7)
+    from xpbd_b200 import _native as N
+    N.check(N.lib().xpbd_mlp_status(C.byref(st), 1), "xpbd_mlp_status")
+    assert st.value == 0
+
+
+@pytest.mark.parametrize("m_rows", [1, 127, 128, 129, 4096 + 77, 300000])
+def test_mlp_inference_tiles(m_rows):
+    """Row counts around the 128-row tile and above the persistent grid
+    (4 CTAs per SM): every row written, rows with weff = 0 get 0."""
+    rng = np.random.default_rng(m_rows)
+    feats = rng.normal(size=(m_rows, 8)).astype(np.float32)
+    weff = rng.uniform(1.0, 10.0, m_rows).astype(np.float32)
+    weff[::7] = 0.0
+    m = WarmStartMLP(seed=4)
+    lam0 = torch.full((m_rows + 5,), 12345.0, device="cuda")
+    m.infer(torch.from_numpy(feats).cuda(), torch.from_numpy(weff).cuda(), m_rows, lam0)
+    got = lam0.cpu().numpy()
+    assert (got[m_rows:] == 12345.0).all()
+    got = got[:m_rows]
+    assert np.isfinite(got).all()
+    assert (got[::7] == 0.0).all()
+    k = min(m_rows, 2000)
+    y = np.zeros(k, np.float32)
+    O.lib().or_mlp_forward(O.fp(np.ascontiguousarray(feats[:k])), k, O.fp(m.w.cpu().numpy()), O.fp(y))
+    ref = np.sign(y) * np.expm1(np.abs(y)) * 1e-3 / np.where(weff[:k] == 0, 1.0, weff[:k])
+    ref[weff[:k] == 0] = 0.0
+    rel = np.abs(got[:k] - ref) / np.maximum(np.abs(ref), 1e-9)
+    assert rel.max() <= 2e-3, rel.max()
 
 
 def test_train_step_entry_point_equals_grads_then_adam():
@@ -309,3 +348,32 @@ def test_warm_start_option_on_the_6dof_solver(ws):
     dy = abs(float(warm.positions()[:, 1].mean() - plain.positions()[:, 1].mean()))
     assert dy < 0.02, dy
     assert warm._runner.substeps_run == 60 * 15
+
+
+@pytest.mark.parametrize("ws", ["previous", "learned"])
+def test_6dof_warm_start_graph_replay_matches_eager_frames(ws):
+    """WarmStartRunner6 replays one captured graph of a frame's substeps from
+    the second frame on; the same frames run eagerly give the same state (to
+    the float atomics' order of the per-phase contact sums), the same manifold
+    point count and the same number of substeps kept warm."""
+    from xpbd_b200.learned import WarmStartRunner6
+    model = WarmStartMLP.pretrained() if ws == "learned" else "previous"
+    kw = dict(dt=1 / 60, substeps=15, iterations=2, floor_y=0.0, friction=0.6, restitution=0.2)
+    a, b = Solver6DOF(**kw), Solver6DOF(**kw)
+    for s in (a, b):
+        scenes.build_box_pile(s, nx=3, ny=2, nz=3, pitch=0.8, y0=0.4)
+    ra, rb = WarmStartRunner6(a, model), WarmStartRunner6(b, model)
+    for f in range(8):
+        ra.step(use_graph=True)
+        rb.step(use_graph=False)
+        if f == 0:
+            assert ra.graph is None
+    torch.cuda.synchronize()
+    assert ra.graph is not None
+    assert ra.substeps_run == rb.substeps_run == 8 * 15
+    assert np.all(np.isfinite(a.positions()))
+    np.testing.assert_allclose(a.positions(), b.positions(), atol=1e-3)
+    np.testing.assert_allclose(a.orientations(), b.orientations(), atol=1e-2)
+    pa, pb = ra.kit.points_total, rb.kit.points_total
+    assert pa > 0 and abs(pa - pb) <= 0.02 * pb, (pa, pb)
+    assert abs(int(ra.learned_used.item()) - int(rb.learned_used.item())) <= 0.1 * 8 * 15

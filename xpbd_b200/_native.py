@@ -96,6 +96,7 @@ _SIGS = {
     "xpbd_scan_i32": ([_p, _p, C.c_int, _p, _p], C.c_int),
     "xpbd3_residual": ([_p, C.c_float, _p, C.c_int, _p, _p, _p], C.c_int),
     "xpbd6_residual": ([_p, _p, _p, C.c_int, _p, _p], C.c_int),
+    "xpbd_mlp_status": ([_ip, C.c_int], C.c_int),
 }
 
 _LIB = None

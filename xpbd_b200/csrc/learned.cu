@@ -1,8 +1,9 @@
 // Learned lambda warm start (no reference counterpart; the reference always
 // restarts every substep from lambda = 0, solver.py:430-431).
 //
-// A small MLP (7 -> 64 -> 64 -> 1, GELU, bf16 weights, fp32 accumulation)
-// predicts, from per-row features at the start of a substep, the multiplier
+// A small MLP (7 -> 64 -> 64 -> 1, GELU, bf16 weights, fp32 accumulation; the
+// first layer's activations are rounded to bf16, the operand of the second
+// layer's tensor-core MMA) predicts, from per-row features at the start of a substep, the multiplier
 // the plain solver converges to.  The prediction seeds lambda and the
 // positions are pre-corrected by the Jacobi-averaged M^-1 grad C^T lambda0, so
 // the iterations start near the fixed point instead of at lambda = 0.
@@ -27,10 +28,13 @@
 //
 // Training: `k_mlp_grads` evaluates the mean squared error of a batch and its
 // gradient with respect to every weight, 64 samples per CTA, all activations in
-// shared memory; `k_adam` updates fp32 master weights and their bf16 copy.
+// shared memory, the first layer's activations rounded to bf16 as in the
+// inference (the gradient passes through the rounding); `k_adam` updates fp32
+// master weights and their bf16 copy.
 #include <cuda_bf16.h>
 
 #include "learned.cuh"
+#include "tc.cuh"
 
 namespace xpbd {
 
@@ -84,33 +88,132 @@ __global__ void k3_features(const float4* x, const float4* v, const int4* ri, co
   }
 }
 
-// ---- inference: one thread per row, bf16 weights widened into shared memory ---------
-__global__ void __launch_bounds__(256) k_mlp_infer(const float* feats, const float* weff, int m,
-                                                   const __nv_bfloat16* wb, float* lam0) {
-  __shared__ float W[kNParam];
-  for (int i = threadIdx.x; i < kNParam; i += blockDim.x) W[i] = __bfloat162float(wb[i]);
+// ---- inference on the tensor cores -------------------------------------------------
+// One CTA (256 threads) per 128-row tile, persistent over tiles.  Layer 1
+// (7 -> 64, fp32 features) runs on the CUDA cores, two threads per row (hidden
+// units 0-31 and 32-63); its GELU outputs are rounded to bf16 and stored as the
+// A operand (128 x 64, K-major core matrices, no swizzle).  Layer 2 (64 -> 64)
+// is one 128 x 64 x 64 bf16 MMA with the fp32 accumulator in tensor memory
+// (four tcgen05.mma of K = 16 issued by one thread, committed to an mbarrier).
+// The epilogue reads the accumulator with tcgen05.ld (warp w: rows 32 (w % 4)..,
+// columns 32 (w / 4)..), adds the bias, applies GELU and the 64 -> 1 output
+// layer; the two half sums of a row meet in shared memory.
+constexpr int kRowsTile = 128;
+constexpr long long kWaitCycles = 1ll << 28;  // bounded mbarrier wait: ~0.14 s, far beyond one MMA
+__device__ int g_mlp_status;                 // 1: a tensor-core wait gave up (rows written as NaN)
+
+// Byte offset of element (row, k) in a K-major operand of 64 columns stored as
+// 8 x 16-byte core matrices: K-adjacent core matrices 128 B apart, row groups 1024 B apart.
+XD uint32_t kmajor_off(int row, int k) {
+  return (uint32_t)((row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__global__ void __launch_bounds__(256) k_mlp_infer_tc(const float* feats, const float* weff, int m,
+                                                      const __nv_bfloat16* wb, float* lam0) {
+  __shared__ __align__(1024) unsigned char sA[kRowsTile * kHid * 2];
+  __shared__ __align__(1024) unsigned char sB[kHid * kHid * 2];
+  __shared__ float sW1[kHid * kIn], sB1[kHid], sB2[kHid], sW3[kHid], sY[kRowsTile];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tbase;
+  __shared__ int gave_up;
+  const int t = threadIdx.x, warp = t >> 5;
+  for (int i = t; i < kHid * kIn; i += blockDim.x) sW1[i] = __bfloat162float(wb[oW1 + i]);
+  for (int i = t; i < kHid; i += blockDim.x) {
+    sB1[i] = __bfloat162float(wb[oB1 + i]);
+    sB2[i] = __bfloat162float(wb[oB2 + i]);
+    sW3[i] = __bfloat162float(wb[oW3 + i]);
+  }
+  // B operand: W2[u][k] (N = u, K = k), K-major
+  for (int i = t; i < kHid * kHid; i += blockDim.x) {
+    const int u = i / kHid, k = i % kHid;
+    *reinterpret_cast<__nv_bfloat16*>(sB + kmajor_off(u, k)) = wb[oW2 + i];
+  }
+  const float b3 = __bfloat162float(wb[oB3]);
+  if (warp == 0) {
+    tc::tmem_alloc(&tbase, 64);
+    tc::tmem_relinquish();
+  }
+  if (t == 0) {
+    tc::mbar_init(&bar, 1);
+    gave_up = 0;
+  }
+  tc::fence_async_smem();
+  tc::fence_before_sync();
   __syncthreads();
-  for (int j = gtid(); j < m; j += gstride()) {
-    float we = weff[j];
-    if (we == 0.0f) {
-      lam0[j] = 0.0f;
-      continue;
-    }
+  tc::fence_after_sync();
+  const uint32_t tmem = tbase;
+  const int r = t & (kRowsTile - 1), h = t >> 7;
+  const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB), idesc = tc::idesc_bf16_f32(kRowsTile, kHid);
+  uint32_t parity = 0;
+  for (int tile = blockIdx.x; (long long)tile * kRowsTile < m; tile += gridDim.x) {
+    const int j = tile * kRowsTile + r;
+    const bool live = j < m;
     float in[kIn];
-    for (int k = 0; k < kIn; ++k) in[k] = feats[(size_t)j * 8 + k];
-    float a1[kHid];
-    for (int u = 0; u < kHid; ++u) {
-      float z = W[oB1 + u];
-      for (int k = 0; k < kIn; ++k) z = __fmaf_rn(W[oW1 + u * kIn + k], in[k], z);
-      a1[u] = gelu(z);
+#pragma unroll
+    for (int k = 0; k < kIn; ++k) in[k] = live ? feats[(size_t)j * 8 + k] : 0.0f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {  // hidden units 32 h + 8 c .. + 7: one 16-byte row of a core matrix
+      uint32_t packed[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float a[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int u = 32 * h + 8 * c + 2 * q + e;
+          float z = sB1[u];
+#pragma unroll
+          for (int k = 0; k < kIn; ++k) z = __fmaf_rn(sW1[u * kIn + k], in[k], z);
+          a[e] = gelu(z);
+        }
+        const __nv_bfloat162 p2 = __floats2bfloat162_rn(a[0], a[1]);
+        packed[q] = *reinterpret_cast<const uint32_t*>(&p2);
+      }
+      *reinterpret_cast<uint4*>(sA + kmajor_off(r, 32 * h + 8 * c)) =
+          make_uint4(packed[0], packed[1], packed[2], packed[3]);
     }
-    float y = W[oB3];
-    for (int u = 0; u < kHid; ++u) {
-      float z = W[oB2 + u];
-      for (int k = 0; k < kHid; ++k) z = __fmaf_rn(W[oW2 + u * kHid + k], a1[k], z);
-      y = __fmaf_rn(W[oW3 + u], gelu(z), y);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < kHid / 16; ++ks)
+        tc::mma_bf16_ss(tmem, tc::smem_desc_kmajor(a0 + ks * 256, 128, 1024),
+                        tc::smem_desc_kmajor(b0 + ks * 256, 128, 1024), idesc, ks > 0);
+      tc::mma_commit(&bar);
     }
-    lam0[j] = slog_inv(y + in[3]) * kLen / we;
+    const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(&bar, parity, kWaitCycles));
+    parity ^= 1u;
+    tc::fence_after_sync();
+    float y = 0.0f;
+    if (ok) {
+      float z[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(32 * h), z);
+#pragma unroll
+      for (int u = 0; u < 32; ++u) y = __fmaf_rn(sW3[32 * h + u], gelu(z[u] + sB2[32 * h + u]), y);
+    } else {
+      gave_up = 1;
+    }
+    if (h == 1) sY[r] = y;
+    tc::fence_before_sync();
+    __syncthreads();
+    const bool failed = gave_up != 0;
+    if (h == 0 && live) {
+      const float we = weff[j];
+      lam0[j] = failed ? __int_as_float(0x7fc00000) : (we == 0.0f ? 0.0f : slog_inv(b3 + y + sY[r] + in[3]) * kLen / we);
+    }
+    if (failed) break;
+  }
+  __syncthreads();
+  if (gave_up) {  // an MMA may still be in flight: give it one more bounded wait before freeing its memory
+    tc::mbar_wait_bounded(&bar, parity ^ 1u, kWaitCycles);
+    if (t == 0) atomicExch(&g_mlp_status, 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, 64);
   }
 }
 
@@ -149,7 +252,7 @@ __global__ void __launch_bounds__(256) k_mlp_grads(const float* feats, const flo
       float z = W[oB1 + u];
       for (int k = 0; k < kIn; ++k) z = __fmaf_rn(W[oW1 + u * kIn + k], X[s * 8 + k], z);
       Z1[i] = z;
-      A1[i] = gelu(z);
+      A1[i] = __bfloat162float(__float2bfloat16_rn(gelu(z)));  // as the inference's bf16 MMA operand
     }
     __syncthreads();
     for (int i = t; i < kTile * kHid; i += T) {  // layer 2
@@ -301,9 +404,22 @@ extern "C" int xpbd_mlp_infer(const float* feats, const float* weff, int m, cons
                               void* stream) {
   if (m < 0 || (m > 0 && (!feats || !weff || !weights_bf16 || !lam0))) return XPBD_ERR_BAD_ARG;
   if (m == 0) return XPBD_OK;
-  k_mlp_infer<<<stream_blocks(m, 256), 256, 0, as_stream(stream)>>>(
+  const int tiles = ceil_div(m, kRowsTile);
+  k_mlp_infer_tc<<<std::min(tiles, 4 * num_sms()), 256, 0, as_stream(stream)>>>(
       feats, weff, m, reinterpret_cast<const __nv_bfloat16*>(weights_bf16), lam0);
   XPBD_LAUNCHED();
+  return XPBD_OK;
+}
+
+// 1 if an inference launch gave up waiting for the tensor core (its rows were
+// written as NaN); `reset` clears the word.  Synchronous.
+extern "C" int xpbd_mlp_status(int* status, int reset) {
+  if (!status) return XPBD_ERR_BAD_ARG;
+  XPBD_CUDA(cudaMemcpyFromSymbol(status, g_mlp_status, sizeof(int)));
+  if (reset) {
+    const int zero = 0;
+    XPBD_CUDA(cudaMemcpyToSymbol(g_mlp_status, &zero, sizeof(int)));
+  }
   return XPBD_OK;
 }
 

@@ -396,7 +396,7 @@ class SubstepKit6:
         self._alloc()
         self.h = s.dt / s.substeps
         self._carry = None
-        self._pair_prev = None
+        self._pair_prev_pending = False  # set by broadphase, consumed by the next begin
         self.np_host = min(s.n_pairs, s.cap)
         # manifold points summed over the substeps begun (the projection count)
         self.points_dev = torch.zeros((), dtype=torch.int64, device=s.device)
@@ -416,7 +416,9 @@ class SubstepKit6:
         self.lam0 = torch.zeros(self.rows, dtype=torch.float32, device=dev)
         self.prev_floor = torch.zeros(self.nf, dtype=torch.float32, device=dev)
         self.prev_pair = torch.zeros(8 * self.cap, dtype=torch.float32, device=dev)
+        self.pair_prev = torch.zeros(8 * self.cap, dtype=torch.float32, device=dev)  # carried across a broad phase
         self.tot_floor = torch.zeros(self.nf, dtype=torch.float32, device=dev)
+        self.slot = torch.arange(self.cap, dtype=torch.int32, device=dev)
 
     @property
     def st(self):
@@ -458,12 +460,13 @@ class SubstepKit6:
         self.np_host = n_new
         keys = T["pairs"][:n_new].long()
         keys = keys[:, 0] * self.n + keys[:, 1]
-        mapped = torch.zeros((self.cap, 8), dtype=torch.float32, device=s.device)
+        mapped = self.pair_prev.view(self.cap, 8)
+        mapped.zero_()
         if n_old and n_new:
             idx = torch.searchsorted(old_keys, keys).clamp_(max=n_old - 1)
             hit = old_keys[idx] == keys
             mapped[:n_new][hit] = old_lam[idx[hit]]
-        self._pair_prev = mapped.view(-1)
+        self._pair_prev_pending = True
 
     def carry(self, lam_rows):
         """Use these per-row multipliers (for example a converged solve's) as the
@@ -479,13 +482,15 @@ class SubstepKit6:
             self._carry = None
         else:
             self.prev_pair.copy_(T["lam_pair"][: 8 * self.cap])
-        if self._pair_prev is not None:  # first substep on a new pair list
-            self.prev_pair.copy_(self._pair_prev)
-            self._pair_prev = None
+        if self._pair_prev_pending:  # first substep on a new pair list
+            self.prev_pair.copy_(self.pair_prev)
+            self._pair_prev_pending = False
         N.check(self.L.xpbd6_integrate(self.st, self.par, self.stream()), "xpbd6_integrate")
         N.check(self.L.xpbd6_manifold(self.st, float(self.s._man_margin), self.stream()), "xpbd6_manifold")
-        if self.np_host:
-            self.points_dev += T["m_hdr"][: self.np_host, 0].sum()
+        # the live pairs' point counts, masked on the device (no host read, so a
+        # captured substep counts the pairs of the frame it is replayed in)
+        live = self.slot < T["n_pairs"].clamp(max=self.cap)
+        self.points_dev += torch.where(live, T["m_hdr"][: self.cap, 0], 0).sum()
         N.check(self.L.xpbd6_features(self.st, self.par, N.ptr(self.prev_floor), N.ptr(self.prev_pair),
                                       N.ptr(self.feats), N.ptr(self.weff), self.stream()), "xpbd6_features")
         self.tot_floor.zero_()
@@ -658,6 +663,8 @@ class WarmStartRunner6:
         self.res_l = torch.zeros(1, dtype=torch.float32, device=dev)
         self.learned_used = torch.zeros(1, dtype=torch.int32, device=dev)
         self.substeps_run = 0
+        self.graph = None
+        self.frames_eager = 0
 
     def _residual(self, out):
         N.check(self.kit.L.xpbd6_residual(C.byref(self.s._st), C.byref(self.s._par), None, 1, N.ptr(out),
@@ -692,10 +699,33 @@ class WarmStartRunner6:
         # substep's.  (A separated manifold point's multiplier is already set
         # to 0 by its solve.)
         kit.prev_floor.mul_((T["lam_floor"][: kit.nf] != 0).to(kit.prev_floor.dtype))
-        self.substeps_run += 1
 
-    def step(self):
-        self.kit.broadphase()  # may grow the pair capacity (a re-bind the kit has absorbed)
-        self.binds = getattr(self.s, "binds", 0)
+    def _frame(self):
         for _ in range(self.s.substeps):
             self._substep()
+
+    def step(self, use_graph=True):
+        """The broad phase, then the frame's substeps: eager in the first frame
+        (which loads every kernel), afterwards one captured CUDA graph of all
+        substeps, replayed every frame.  The substeps read no host value that
+        changes between frames (the pair count is masked on the device, the
+        carried pair multipliers sit in a persistent buffer), so one capture
+        serves every frame until the pair capacity grows or the solver is
+        re-bound, which re-captures."""
+        cap = self.kit.cap
+        self.kit.broadphase()  # may grow the pair capacity (a re-bind the kit has absorbed)
+        binds = getattr(self.s, "binds", 0)
+        if binds != self.binds or self.kit.cap != cap:
+            self.graph = None
+        self.binds = binds
+        if not use_graph or self.frames_eager == 0:
+            self._frame()
+            self.frames_eager += 1
+        else:
+            if self.graph is None:
+                self.graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(self.graph):  # records only: the frame runs in the replay
+                    self._frame()
+            self.kit._pair_prev_pending = False  # consumed by the replayed first substep
+            self.graph.replay()
+        self.substeps_run += self.s.substeps
