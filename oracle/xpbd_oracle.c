@@ -1325,8 +1325,11 @@ static float or_gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118
 
 /* The first layer's activations are rounded to bf16, as the engine does for
  * the operand of its tensor-core second layer (the gradient passes straight
- * through the rounding).  or_mlp_round_activations(0) turns the rounding off,
- * so that finite differences of the loss can check the gradient formulas. */
+ * through the rounding), and so is the gradient at the second layer's input
+ * dL/dz2, the operand of the engine's two backward tensor-core products (dL/da1
+ * and dL/dW2; the bias gradient uses the same rounded values).
+ * or_mlp_round_activations(0) turns both roundings off, so that finite
+ * differences of the loss can check the gradient formulas. */
 static int or_mlp_act_bf16 = 1;
 void or_mlp_round_activations(int on) { or_mlp_act_bf16 = on; }
 static float or_act(float a) { return or_mlp_act_bf16 ? or_bf16_round(a) : a; }
@@ -1367,7 +1370,8 @@ double or_mlp_grads(const float *feats, const float *targets, int B, const float
         double dz2[MLP_H], dz1[MLP_H];
         for (int u = 0; u < MLP_H; ++u) {
             G3[u] += dy * a2[u];
-            dz2[u] = dy * W3[u] * or_gelu_d(z2[u]);
+            dz2[u] = or_mlp_act_bf16 ? (double)or_bf16_round((float)dy * W3[u] * or_gelu_d(z2[u]))
+                                     : dy * W3[u] * or_gelu_d(z2[u]);
         }
         GB3[0] += dy;
         for (int u = 0; u < MLP_H; ++u) {

@@ -26,11 +26,13 @@
 // nothing), and lambda0 = slog^-1(y) 1 mm / (w + alpha~).  For the 6-DOF
 // contact rows (xpbd6.cu) the same features and the same network are used.
 //
-// Training: `k_mlp_grads` evaluates the mean squared error of a batch and its
-// gradient with respect to every weight, 64 samples per CTA, all activations in
-// shared memory, the first layer's activations rounded to bf16 as in the
-// inference (the gradient passes through the rounding); `k_adam` updates fp32
-// master weights and their bf16 copy.
+// Training: `k_mlp_grads_tc` evaluates the mean squared error of a batch and
+// its gradient with respect to every weight, 128 samples per tile, the three
+// 64-wide products (forward, input gradient, weight gradient) on the tensor
+// cores with bf16 operands (the first layer's activations and the gradient at
+// the second layer's input, rounded as the oracle does; the gradient passes
+// straight through the roundings) and fp32 accumulators in tensor memory;
+// `k_adam` updates fp32 master weights and their bf16 copy.
 #include <cuda_bf16.h>
 
 #include "learned.cuh"
@@ -217,110 +219,285 @@ __global__ void __launch_bounds__(256) k_mlp_infer_tc(const float* feats, const 
   }
 }
 
-// ---- training: loss and gradient of a batch ----------------------------------------
-// 64 samples per CTA (256 threads); activations in shared memory; per-CTA weight
-// gradients are summed in shared memory and added to G with one atomic each.
-constexpr int kTile = 64;
+// ---- training: loss and gradient of a batch, on the tensor cores --------------------
+// One CTA (256 threads, one per SM) per 128-sample tile, persistent over tiles.
+// Thread (r, h) = (t % 128, t / 128) owns sample r of the tile and hidden units
+// 32 h .. 32 h + 31.  Per tile:
+//   1. layer 1 on the CUDA cores; a1 = bf16(GELU(z1)) stored twice, as A of the
+//      forward product ([s][k], K = k) and as B of the weight gradient ([k][s], K = s);
+//   2. z2 = a1 W2^T: one 128 x 64 x 64 MMA (tensor memory columns 0..63);
+//   3. output, error e, dy = e / B; dz2 = bf16(dy W3 gelu'(z2)) stored as A of
+//      the input gradient ([s][u]) and as A of the weight gradient ([u][s], rows
+//      64..127 zero); dy a2 kept in shared memory for dL/dW3;
+//   4. da1 = dz2 W2: one 128 x 64 x 64 MMA (columns 64..127, B = W2^T), and
+//      dW2 += dz2^T a1: 128 x 64 x 128 (columns 128..191, accumulated over the
+//      CTA's tiles; rows 64..127 stay zero);
+//   5. dz1 = da1 gelu'(z1) and the small gradients (W1, b1, b2, W3, b3) summed
+//      over the tile's samples from shared memory.
+// At the end every CTA adds its gradient into G (one atomic per weight) and its
+// loss share into `loss`.
+constexpr int kT = 128;
+// Byte offset of element (row, k) of a K-major operand of 128 columns (K = 128).
+XD uint32_t kmajor128_off(int row, int k) {
+  return (uint32_t)((row >> 3) * 2048 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+XD __nv_bfloat16 bf16r(float x) { return __float2bfloat16_rn(x); }
 
-__global__ void __launch_bounds__(256) k_mlp_grads(const float* feats, const float* targets, int B,
-                                                   const __nv_bfloat16* wb, float* G, float* loss) {
-  extern __shared__ float sm[];
-  float* W = sm;                          // kNParam
-  float* g = W + kNParam;                 // kNParam
-  float* X = g + kNParam;                 // kTile * 8
-  float* Z1 = X + kTile * 8;              // kTile * 64
-  float* A1 = Z1 + kTile * kHid;          // kTile * 64
-  float* Z2 = A1 + kTile * kHid;          // kTile * 64 (then dZ2)
-  float* DZ1 = Z2 + kTile * kHid;         // kTile * 64
-  float* DY = DZ1 + kTile * kHid;         // kTile
-  const int t = threadIdx.x, T = blockDim.x;
-  for (int i = t; i < kNParam; i += T) {
-    W[i] = __bfloat162float(wb[i]);
-    g[i] = 0.0f;
+struct GradSmem {  // byte offsets into the dynamic shared memory (base aligned to 1024)
+  static constexpr uint32_t A1 = 0;                  // [s][k] bf16, K = 64
+  static constexpr uint32_t DZ2 = A1 + 16384;        // [s][u] bf16, K = 64
+  static constexpr uint32_t DZ2T = DZ2 + 16384;      // [u][s] bf16, K = 128, 128 rows (64..127 zero)
+  static constexpr uint32_t A1T = DZ2T + 32768;      // [k][s] bf16, K = 128
+  static constexpr uint32_t W2 = A1T + 16384;        // [u][k] bf16
+  static constexpr uint32_t W2T = W2 + 8192;         // [k][u] bf16
+  static constexpr uint32_t F = W2T + 8192;          // fp32 [s][64]: dy a2, then dz1
+  static constexpr uint32_t GACC = F + 32768;        // fp32 [kNParam] (the W2 block unused)
+  static constexpr uint32_t WF = GACC + 4 * 4740;    // fp32 W1 (448), b1, b2, W3 (64 each)
+  static constexpr uint32_t X = WF + 4 * 640;        // fp32 [s][8]
+  static constexpr uint32_t TGT = X + 4 * kT * 8;    // fp32 [s]
+  static constexpr uint32_t YP = TGT + 4 * kT;       // fp32 [2][s]
+  static constexpr uint32_t BAR = YP + 4 * 2 * kT;   // mbarrier (8 B), tmem base, gave_up
+  static constexpr uint32_t TOTAL = BAR + 64;
+};
+
+__global__ void __launch_bounds__(256, 1) k_mlp_grads_tc(const float* feats, const float* targets, int B,
+                                                         const __nv_bfloat16* wb, float* G, float* loss) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  using S = GradSmem;
+  float* sF = reinterpret_cast<float*>(sm + S::F);
+  float* gacc = reinterpret_cast<float*>(sm + S::GACC);
+  float* sW1 = reinterpret_cast<float*>(sm + S::WF);
+  float* sB1 = sW1 + kHid * kIn;
+  float* sB2 = sB1 + kHid;
+  float* sW3 = sB2 + kHid;
+  float* sX = reinterpret_cast<float*>(sm + S::X);
+  float* sT = reinterpret_cast<float*>(sm + S::TGT);
+  float* sYp = reinterpret_cast<float*>(sm + S::YP);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + S::BAR);
+  uint32_t* tbase = reinterpret_cast<uint32_t*>(sm + S::BAR + 8);
+  int* gave_up = reinterpret_cast<int*>(sm + S::BAR + 12);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  for (int i = t; i < kHid * kIn; i += blockDim.x) sW1[i] = __bfloat162float(wb[oW1 + i]);
+  for (int i = t; i < kHid; i += blockDim.x) {
+    sB1[i] = __bfloat162float(wb[oB1 + i]);
+    sB2[i] = __bfloat162float(wb[oB2 + i]);
+    sW3[i] = __bfloat162float(wb[oW3 + i]);
   }
+  for (int i = t; i < kNParam; i += blockDim.x) gacc[i] = 0.0f;
+  for (int i = t; i < 32768 / 16; i += blockDim.x) reinterpret_cast<uint4*>(sm + S::DZ2T)[i] = make_uint4(0, 0, 0, 0);
+  for (int i = t; i < kHid * kHid; i += blockDim.x) {
+    const int u = i / kHid, k = i % kHid;
+    *reinterpret_cast<__nv_bfloat16*>(sm + S::W2 + kmajor_off(u, k)) = wb[oW2 + i];
+    *reinterpret_cast<__nv_bfloat16*>(sm + S::W2T + kmajor_off(k, u)) = wb[oW2 + i];
+  }
+  const float b3 = __bfloat162float(wb[oB3]);
+  if (warp == 0) {
+    tc::tmem_alloc(tbase, 256);
+    tc::tmem_relinquish();
+  }
+  if (t == 0) {
+    tc::mbar_init(bar, 1);
+    *gave_up = 0;
+  }
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tbase;
+  const int r = t & (kT - 1), h = t >> 7;
+  const uint32_t lanes = (uint32_t)(32 * (warp & 3)) << 16;
+  const uint32_t s0 = tc::smem_u32(sm);
+  const uint32_t idesc = tc::idesc_bf16_f32(kT, kHid);
+  const float invB = 1.0f / (float)B;
+  uint32_t parity = 0;
+  int tiles_done = 0;
   float lsum = 0.0f;
-  for (int base = blockIdx.x * kTile; base < B; base += gridDim.x * kTile) {
-    const int ns = min(kTile, B - base);
-    __syncthreads();
-    for (int i = t; i < kTile * 8; i += T) {
-      int s = i / 8;
-      X[i] = s < ns ? feats[(size_t)(base + s) * 8 + (i % 8)] : 0.0f;
+  auto wait_mma = [&]() {
+    const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(bar, parity, kWaitCycles));
+    parity ^= 1u;
+    tc::fence_after_sync();
+    if (!ok) *gave_up = 1;
+    return ok;
+  };
+  for (int tile = blockIdx.x; (long long)tile * kT < B; tile += gridDim.x) {
+    const int j = tile * kT + r;
+    const bool live = j < B;
+    float x[kIn];
+#pragma unroll
+    for (int k = 0; k < kIn; ++k) x[k] = live ? feats[(size_t)j * 8 + k] : 0.0f;
+    if (h == 0) {
+#pragma unroll
+      for (int k = 0; k < kIn; ++k) sX[r * 8 + k] = x[k];
+      sT[r] = live ? targets[j] : 0.0f;
     }
-    __syncthreads();
-    for (int i = t; i < kTile * kHid; i += T) {  // layer 1
-      int s = i / kHid, u = i % kHid;
-      float z = W[oB1 + u];
-      for (int k = 0; k < kIn; ++k) z = __fmaf_rn(W[oW1 + u * kIn + k], X[s * 8 + k], z);
-      Z1[i] = z;
-      A1[i] = __bfloat162float(__float2bfloat16_rn(gelu(z)));  // as the inference's bf16 MMA operand
+    // 1. layer 1: a1 of units 32 h .. 32 h + 31, as [s][k] (16-byte rows) and [k][s]
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      uint32_t packed[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        __nv_bfloat16 a[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int u = 32 * h + 8 * c + 2 * q + e;
+          float z = sB1[u];
+#pragma unroll
+          for (int k = 0; k < kIn; ++k) z = __fmaf_rn(sW1[u * kIn + k], x[k], z);
+          a[e] = bf16r(gelu(z));
+          *reinterpret_cast<__nv_bfloat16*>(sm + S::A1T + kmajor128_off(u, r)) = a[e];
+        }
+        __nv_bfloat162 p2;
+        p2.x = a[0];
+        p2.y = a[1];
+        packed[q] = *reinterpret_cast<const uint32_t*>(&p2);
+      }
+      *reinterpret_cast<uint4*>(sm + S::A1 + kmajor_off(r, 32 * h + 8 * c)) =
+          make_uint4(packed[0], packed[1], packed[2], packed[3]);
     }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
     __syncthreads();
-    for (int i = t; i < kTile * kHid; i += T) {  // layer 2
-      int s = i / kHid, u = i % kHid;
-      float z = W[oB2 + u];
-      for (int k = 0; k < kHid; ++k) z = __fmaf_rn(W[oW2 + u * kHid + k], A1[s * kHid + k], z);
-      Z2[i] = z;
+    // 2. z2 = a1 W2^T
+    if (t == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < kHid / 16; ++ks)
+        tc::mma_bf16_ss(tmem, tc::smem_desc_kmajor(s0 + S::A1 + ks * 256, 128, 1024),
+                        tc::smem_desc_kmajor(s0 + S::W2 + ks * 256, 128, 1024), idesc, ks > 0);
+      tc::mma_commit(bar);
     }
-    __syncthreads();
-    for (int s = t; s < kTile; s += T) {  // output + loss
-      float y = W[oB3];
-      for (int u = 0; u < kHid; ++u) y = __fmaf_rn(W[oW3 + u], gelu(Z2[s * kHid + u]), y);
-      float e = s < ns ? (y + X[s * 8 + 3]) - targets[base + s] : 0.0f;
-      lsum += e * e;
-      DY[s] = e / (float)B;  // d(mean 0.5 e^2)/dy... scaled below
+    float z2[32], a2[32];
+    float yp = 0.0f;
+    if (wait_mma()) {
+      tc::tmem_ld32(tmem + lanes + (uint32_t)(32 * h), z2);
+#pragma unroll
+      for (int u = 0; u < 32; ++u) {
+        z2[u] += sB2[32 * h + u];
+        a2[u] = gelu(z2[u]);
+        yp = __fmaf_rn(sW3[32 * h + u], a2[u], yp);
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < 32; ++u) z2[u] = a2[u] = 0.0f;
     }
+    sYp[h * kT + r] = yp;
     __syncthreads();
-    for (int i = t; i < kHid; i += T) {  // dW3, db3 (i == 0)
+    if (*gave_up) break;
+    // 3. output, error, dz2
+    const float y = (b3 + sYp[r]) + sYp[kT + r];
+    const float e = live ? (y + x[3]) - sT[r] : 0.0f;
+    const float dy = e * invB;
+    if (h == 0) lsum += e * e;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      uint32_t packed[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        __nv_bfloat16 d[2];
+#pragma unroll
+        for (int e2 = 0; e2 < 2; ++e2) {
+          const int i = 8 * c + 2 * q + e2, u = 32 * h + i;
+          d[e2] = bf16r(dy * sW3[u] * gelu_d(z2[i]));
+          sF[r * kHid + u] = dy * a2[i];
+          *reinterpret_cast<__nv_bfloat16*>(sm + S::DZ2T + kmajor128_off(u, r)) = d[e2];
+        }
+        __nv_bfloat162 p2;
+        p2.x = d[0];
+        p2.y = d[1];
+        packed[q] = *reinterpret_cast<const uint32_t*>(&p2);
+      }
+      *reinterpret_cast<uint4*>(sm + S::DZ2 + kmajor_off(r, 32 * h + 8 * c)) =
+          make_uint4(packed[0], packed[1], packed[2], packed[3]);
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    // 4. da1 = dz2 W2 (columns 64..127), dW2 += dz2^T a1 (columns 128..191)
+    if (t == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < kHid / 16; ++ks)
+        tc::mma_bf16_ss(tmem + 64, tc::smem_desc_kmajor(s0 + S::DZ2 + ks * 256, 128, 1024),
+                        tc::smem_desc_kmajor(s0 + S::W2T + ks * 256, 128, 1024), idesc, ks > 0);
+#pragma unroll
+      for (int ks = 0; ks < kT / 16; ++ks)
+        tc::mma_bf16_ss(tmem + 128, tc::smem_desc_kmajor(s0 + S::DZ2T + ks * 256, 128, 2048),
+                        tc::smem_desc_kmajor(s0 + S::A1T + ks * 256, 128, 2048), idesc, tiles_done > 0 || ks > 0);
+      tc::mma_commit(bar);
+    }
+    // the tile's sums for W3, b2, b3 while the tensor core works
+    if (t < kHid) {
       float acc = 0.0f;
-      for (int s = 0; s < kTile; ++s) acc = __fmaf_rn(DY[s], gelu(Z2[s * kHid + i]), acc);
-      g[oW3 + i] += acc;
-      if (i == 0) {
-        float b = 0.0f;
-        for (int s = 0; s < kTile; ++s) b += DY[s];
-        g[oB3] += b;
+      for (int s = 0; s < kT; ++s) acc += sF[s * kHid + t];
+      gacc[oW3 + t] += acc;
+    } else if (t < 2 * kHid) {
+      const int u = t - kHid;
+      float acc = 0.0f;
+      for (int s = 0; s < kT; ++s)
+        acc += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(sm + S::DZ2 + kmajor_off(s, u)));
+      gacc[oB2 + u] += acc;
+    }
+    if (h == 0) {
+      float d = dy;
+      for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+      if (lane == 0) atomicAdd(gacc + oB3, d);
+    }
+    __syncthreads();  // sF is rewritten below
+    ++tiles_done;
+    if (wait_mma()) {
+      float da1[32];
+      tc::tmem_ld32(tmem + lanes + 64u + (uint32_t)(32 * h), da1);
+      // 5. dz1 = da1 gelu'(z1), z1 recomputed as in step 1
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int u = 32 * h + i;
+        float z = sB1[u];
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) z = __fmaf_rn(sW1[u * kIn + k], x[k], z);
+        sF[r * kHid + u] = da1[i] * gelu_d(z);
       }
     }
+    tc::fence_before_sync();
     __syncthreads();
-    for (int i = t; i < kTile * kHid; i += T) {  // dZ2 (overwrites Z2)
-      int u = i % kHid;
-      float z = Z2[i];
-      Z2[i] = DY[i / kHid] * W[oW3 + u] * gelu_d(z);
-    }
-    __syncthreads();
-    for (int i = t; i < kHid * kHid; i += T) {  // dW2[u][k] = sum_s dZ2[s][u] A1[s][k]
-      int u = i / kHid, k = i % kHid;
+    if (*gave_up) break;
+    for (int o = t; o < kHid * kIn + kHid; o += blockDim.x) {
       float acc = 0.0f;
-      for (int s = 0; s < kTile; ++s) acc = __fmaf_rn(Z2[s * kHid + u], A1[s * kHid + k], acc);
-      g[oW2 + i] += acc;
+      if (o < kHid * kIn) {
+        const int u = o / kIn, k = o % kIn;
+        for (int s = 0; s < kT; ++s) acc = __fmaf_rn(sF[s * kHid + u], sX[s * 8 + k], acc);
+        gacc[oW1 + o] += acc;
+      } else {
+        const int u = o - kHid * kIn;
+        for (int s = 0; s < kT; ++s) acc += sF[s * kHid + u];
+        gacc[oB1 + u] += acc;
+      }
     }
-    for (int u = t; u < kHid; u += T) {
-      float acc = 0.0f;
-      for (int s = 0; s < kTile; ++s) acc += Z2[s * kHid + u];
-      g[oB2 + u] += acc;
-    }
-    for (int i = t; i < kTile * kHid; i += T) {  // dZ1[s][k] = gelu'(Z1) sum_u W2[u][k] dZ2[s][u]
-      int s = i / kHid, k = i % kHid;
-      float acc = 0.0f;
-      for (int u = 0; u < kHid; ++u) acc = __fmaf_rn(W[oW2 + u * kHid + k], Z2[s * kHid + u], acc);
-      DZ1[i] = acc * gelu_d(Z1[i]);
-    }
-    __syncthreads();
-    for (int i = t; i < kHid * kIn; i += T) {  // dW1[u][k] = sum_s dZ1[s][u] X[s][k]
-      int u = i / kIn, k = i % kIn;
-      float acc = 0.0f;
-      for (int s = 0; s < kTile; ++s) acc = __fmaf_rn(DZ1[s * kHid + u], X[s * 8 + k], acc);
-      g[oW1 + i] += acc;
-    }
-    for (int u = t; u < kHid; u += T) {
-      float acc = 0.0f;
-      for (int s = 0; s < kTile; ++s) acc += DZ1[s * kHid + u];
-      g[oB1 + u] += acc;
-    }
+    __syncthreads();  // sX, sT and sF are rewritten by the next tile
   }
   __syncthreads();
-  for (int i = t; i < kNParam; i += T) atomicAdd(G + i, g[i]);
+  const bool failed = *gave_up != 0;
+  if (failed) {  // an MMA may still be in flight: one more bounded wait before its memory is freed
+    tc::mbar_wait_bounded(bar, parity ^ 1u, kWaitCycles);
+  } else if (tiles_done > 0 && (warp & 3) < 2) {  // dW2 rows u = 0..63 live in lanes 0..63
+    float v[32];
+    tc::tmem_ld32(tmem + lanes + 128u + (uint32_t)(32 * h), v);
+    const int u = 32 * (warp & 3) + lane;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) atomicAdd(G + oW2 + u * kHid + 32 * h + i, v[i]);
+  }
+  if (!failed) {
+    for (int i = t; i < kNParam; i += blockDim.x)
+      if (i < oW2 || i >= oB2) atomicAdd(G + i, gacc[i]);
+  }
   for (int o = 16; o; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-  if ((t & 31) == 0) atomicAdd(loss, lsum / (float)B);
+  if (lane == 0) atomicAdd(loss, failed ? __int_as_float(0x7fc00000) : lsum * invB);
+  if (failed && t == 0) atomicExch(&g_mlp_status, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, 256);
+  }
 }
 
 // Adam (Kingma & Ba 2015) on fp32 master weights; writes the bf16 copy and clears G.
@@ -423,7 +600,7 @@ extern "C" int xpbd_mlp_status(int* status, int reset) {
   return XPBD_OK;
 }
 
-static size_t grads_smem() { return sizeof(float) * (2 * kNParam + kTile * 8 + 4 * kTile * kHid + kTile); }
+static size_t grads_smem() { return GradSmem::TOTAL; }
 
 extern "C" int xpbd_mlp_grads(const float* feats, const float* targets, int B, const void* weights_bf16, float* G,
                               float* loss, void* stream) {
@@ -431,12 +608,12 @@ extern "C" int xpbd_mlp_grads(const float* feats, const float* targets, int B, c
   cudaStream_t st = as_stream(stream);
   static bool attr = false;
   if (!attr) {
-    XPBD_CUDA(cudaFuncSetAttribute(k_mlp_grads, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grads_smem()));
+    XPBD_CUDA(cudaFuncSetAttribute(k_mlp_grads_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grads_smem()));
     attr = true;
   }
   XPBD_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), st));
-  int blocks = std::min(ceil_div(B, kTile), 2 * num_sms());
-  k_mlp_grads<<<blocks, 256, grads_smem(), st>>>(feats, targets, B, reinterpret_cast<const __nv_bfloat16*>(weights_bf16),
+  int blocks = std::min(ceil_div(B, kT), num_sms());
+  k_mlp_grads_tc<<<blocks, 256, grads_smem(), st>>>(feats, targets, B, reinterpret_cast<const __nv_bfloat16*>(weights_bf16),
                                                  G, loss);
   XPBD_LAUNCHED();
   return XPBD_OK;

@@ -2,6 +2,7 @@
 
     python -m xpbd_b200.train_warm_start --samples 10000000 --out weights.npy
     python -m xpbd_b200.train_warm_start --eval weights.npy
+    python -m xpbd_b200.train_warm_start --time-infer [ROWS ...]
 
 Data (half from each family, by sample count):
   * randomized cloths (n x n, n ~ U{32..128}; spacing 0.02 m, 0.01 kg, two
@@ -188,6 +189,22 @@ def _event_ms(fn, reps=20):
     return e0.elapsed_time(e1) / reps
 
 
+def time_inference(m, rows_list=(2400, 14897, 113410, 1 << 20), reps=50, seed=0):
+    """Device time of one ``xpbd_mlp_infer`` launch (tensor-core inference) per
+    row count, on random features (mean of `reps` launches, CUDA events)."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    for R in rows_list:
+        feats = torch.from_numpy(rng.normal(size=(R, 8)).astype(np.float32)).cuda()
+        weff = torch.from_numpy(rng.uniform(1.0, 10.0, R).astype(np.float32)).cuda()
+        lam = torch.zeros(R, device="cuda")
+        us = _event_ms(lambda: m.infer(feats, weff, R, lam), reps=reps) * 1e3
+        if not bool(torch.isfinite(lam).all()):
+            raise RuntimeError("non-finite inference output")
+        out[str(R)] = {"us": round(us, 2), "rows_per_s": round(R / (us * 1e-6), 1)}
+    return out
+
+
 def time_warm_start(m):
     """Device time of the warm start's extra work per substep (features +
     inference + warm apply) against one plain Jacobi iteration (solve + apply),
@@ -292,8 +309,14 @@ def main():
     ap.add_argument("--out", default=None, help="save the trained weights (float32 .npy)")
     ap.add_argument("--eval", default=None, help="evaluate saved weights instead of training")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--time-infer", type=int, nargs="*", default=None, metavar="ROWS",
+                    help="only time the inference launch at these row counts (shipped weights)")
     a = ap.parse_args()
     report = {}
+    if a.time_infer is not None:
+        m = WarmStartMLP.pretrained()
+        print(json.dumps(time_inference(m, tuple(a.time_infer) or (2400, 14897, 113410, 1 << 20))))
+        return
     if a.eval:
         m = WarmStartMLP()
         m.load_weights(a.eval)
