@@ -141,6 +141,41 @@ def test_lbvh_pairs_match_oracle_both_paths(dims):
     np.testing.assert_array_equal(eng.pairs(), np.stack([orc.pair_a[:k], orc.pair_b[:k]], 1))
 
 
+@pytest.mark.parametrize("count", [2, 3, 97, 600])
+def test_fused_lbvh_dense_overlap_matches_oracle(count):
+    """Every box overlapping nearly every other (a tight random cloud): each
+    query walks most of the tree, so the fused broad phase's shared frontier of
+    64 nodes per 8-lane group overflows and the overflowing children are walked
+    by single lanes.  The pair set must still equal the oracle's, sorted by
+    (a, b); 2 and 3 bodies are the smallest trees."""
+    rng = np.random.default_rng(count)
+    kw = dict(substeps=15, iterations=2, floor_y=-10.0, friction=0.6, restitution=0.2, broadphase="lbvh")
+    boxes = []
+    for _ in range(count):
+        q = rng.normal(size=4)
+        boxes.append((tuple(rng.uniform(-0.3, 0.3, 3)), tuple(rng.uniform(0.2, 0.4, 3)), tuple(q / np.linalg.norm(q))))
+
+    def build(s):
+        for x, he, q in boxes:
+            s.add_box(x, he, 1.0, quaternion=q)
+
+    eng, orc = _pair(build, **kw)
+    eng._flush()
+    orc._flush()
+    N.check(lib6().xpbd6_broadphase(eng._h, N.stream_of(eng.device)))
+    if eng.n_pairs > eng.cap:
+        eng._alloc_pairs(int(eng.n_pairs * 1.5))
+        eng._bind()
+        eng.status()
+        N.check(lib6().xpbd6_broadphase(eng._h, N.stream_of(eng.device)))
+    assert eng.status() == 0
+    k = orc._broadphase()
+    assert eng.n_pairs == k
+    if count >= 97:
+        assert k > 0.8 * count * (count - 1) / 2
+    np.testing.assert_array_equal(eng.pairs(), np.stack([orc.pair_a[:k], orc.pair_b[:k]], 1))
+
+
 def test_body_aabb_and_morton_bit_exact(golden):
     g = golden("pairs1440_lbvh")
     s = Solver6DOF(device="cuda:0", substeps=15, iterations=2, broadphase="lbvh")

@@ -1527,7 +1527,8 @@ __global__ void k6_pairs_write(Dev6 s, BP6 b, int* status) {
 // j, bodies are in ascending order).
 // =================================================================================
 constexpr int kFusedMaxBoxes = 2048;
-constexpr int kFrontierRounds = 3;  // 2^3 = 8 lanes per query
+constexpr int kFront = 64;  // frontier entries per 8-lane group (in the sort's shared memory)
+static_assert(sizeof(BlockSortSmem) >= sizeof(int) * (1024 / 8) * kFront, "frontier does not fit");
 
 // Shared memory: lo, hi (2 x 16 n), region A (32 n: sort keys + ping-pong
 // during the sort and build, internal-node bounds afterwards), child (8 n),
@@ -1676,10 +1677,9 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
     }
   }
   __syncthreads();
-  // 6. queries (kernels_bvh.py:52-85): eight lanes per body, each walking one
-  // of the (up to eight) subtrees three levels below the root.  A node's
-  // bounds contain its leaves', so the pairs found are exactly those of a walk
-  // from the root.
+  // 6. queries (kernels_bvh.py:52-85): eight lanes per body walking the tree
+  // together (below).  A node's bounds contain its leaves', so the pairs found
+  // are exactly those of a single walk from the root.
   // keep_pair (kernels_bvh.py:74-83) from the w lanes of the AABBs (one scene)
   auto keep = [&](int i, int j) {
     if (!(j > i)) return false;
@@ -1735,20 +1735,72 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
   const int l = tid & 7, G = tid >> 3, NG = T >> 3;
   const unsigned full = 0xffffffffu;
   const int lead = (tid & 31) & ~7;
-  // lane l's subtree: three levels down from the root along the bits of l
-  // (most significant first); a lane whose path reaches a leaf early owns it
-  // only if its remaining bits are zero, so the subtrees are disjoint and
-  // cover every leaf
-  int my_start = 0;
-  for (int d = 0; d < kFrontierRounds && my_start >= 0; ++d) {
-    const int bit = (l >> (kFrontierRounds - 1 - d)) & 1;
-    if (my_start < n - 1) {
-      int2 c = child[my_start];
-      my_start = bit ? c.y : c.x;
-    } else if (bit) {
-      my_start = -1;
+  // Cooperative walk: the group's eight lanes share one frontier of internal
+  // nodes whose bounds overlap the query (in the sort's shared memory, dead
+  // after the sort).  Each round every lane takes one node off the top, tests
+  // its two children, emits the overlapping leaves that pass the filter and
+  // pushes the overlapping internal children (a prefix sum over the lanes gives
+  // their slots).  So a round costs one node visit whatever the tree's shape,
+  // and the lanes share the work of a query wherever it lies.  A child that no
+  // longer fits in the frontier is walked by its lane alone (`query_from`).
+  // The rounds depend only on the tree and the query, so a second walk of the
+  // same body repeats each lane's emissions exactly.
+  const unsigned gmask = 0xffu << lead;
+  int* front = reinterpret_cast<int*>(&sort_sm) + G * kFront;
+  auto group_query = [&](int i, auto emit) {
+    if (n < 2) return;
+    const float4 qlo = LO[i], qhi = HI[i];
+    int cnt = overlaps(qlo, qhi, INLO[0], INHI[0]) ? 1 : 0;
+    if (l == 0) front[0] = 0;  // the root
+    __syncwarp(gmask);
+    for (int rounds = 0; cnt > 0; ++rounds) {
+      if (rounds >= n) {  // every internal node is pushed at most once
+        raise_status(status, XPBD_ERR_BAD_INDEX);
+        break;
+      }
+      const int take = min(cnt, 8);
+      const int node = l < take ? front[cnt - 1 - l] : -1;
+      cnt -= take;
+      __syncwarp(gmask);  // the pops are read before the pushes overwrite them
+      int push[2], np = 0;
+      if (node >= 0) {
+        if (node >= n - 1) {
+          raise_status(status, XPBD_ERR_BAD_INDEX);
+        } else {
+          const int2 c = child[node];
+          const int ch[2] = {c.x, c.y};
+          for (int e = 0; e < 2; ++e) {
+            const int x = ch[e];
+            if (x < 0 || x >= 2 * n - 1) {
+              raise_status(status, XPBD_ERR_BAD_INDEX);
+              continue;
+            }
+            if (!overlaps(qlo, qhi, qlo_of(x), qhi_of(x))) continue;
+            if (x >= n - 1) {
+              const int j = (int)vals[x - (n - 1)];
+              if (keep(i, j)) emit(j);
+            } else {
+              push[np++] = x;
+            }
+          }
+        }
+      }
+      int ex = np;
+      for (int o = 1; o < 8; o <<= 1) {
+        const int y = __shfl_up_sync(gmask, ex, o, 8);
+        if (l >= o) ex += y;
+      }
+      const int tot = __shfl_sync(gmask, ex, lead + 7);
+      ex -= np;
+      for (int q = 0; q < np; ++q) {
+        const int pos = cnt + ex + q;
+        if (pos < kFront) front[pos] = push[q];
+        else query_from(i, push[q], emit);
+      }
+      cnt = min(cnt + tot, kFront);
+      __syncwarp(gmask);
     }
-  }
+  };
   // bodies interleaved over the cluster (i = rank + csize k), so the dense
   // parts of a scene spread over every CTA; the k-th body of this CTA goes to
   // group k mod NG
@@ -1759,7 +1811,7 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
   // sorts them), so a body whose pairs fit is written without a second walk.
   auto count_body = [&](int i) {
     int c = 0;
-    query_from(i, my_start, [&](int j) {
+    group_query(i, [&](int j) {
       if (gper == 1) {
         const int slot = atomicAdd(&s_fill[G], 1);
         if (slot < kStagePairs) stage_all[G * kStagePairs + slot] = j;
@@ -1817,9 +1869,9 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
       const int base = live ? offs[i] : 0;
       const bool staged = body_total <= kStagePairs;
       const bool prestaged = staged && gper == 1;  // the count walk filled the stage already
-      if (live && c > 0 && !prestaged) {
+      if (live && body_total > 0 && !prestaged) {  // the whole group walks again
         int r = 0;
-        query_from(i, my_start, [&](int j) {
+        group_query(i, [&](int j) {
           if (staged) stage[ex + r] = j;
           else if (base + ex + r < s.cap) s.pairs[base + ex + r] = make_int2(i, j);
           ++r;
