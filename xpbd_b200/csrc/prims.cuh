@@ -75,20 +75,14 @@ XD void block_sort_pairs_u64(BlockSortSmem& S, uint64_t* k0, uint32_t* v0, uint6
       const unsigned rank = __popc(peers & ((1u << lane) - 1u));
       if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
       __syncthreads();
-      // exclusive scan of each digit's column over the 32 warps: warp w takes
-      // digits 8w .. 8w + 7, lane = source warp (row stride 257: no bank conflicts)
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int dq = warp * 8 + q;
-        const unsigned c = wcnt[lane][dq];
-        unsigned inc = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const unsigned y = __shfl_up_sync(kFull, inc, o);
-          if (lane >= o) inc += y;
+      if (tid < 256) {
+        unsigned run = 0;
+        for (int w = 0; w < 32; ++w) {
+          unsigned c = wcnt[w][tid];
+          wcnt[w][tid] = run;
+          run += c;
         }
-        wcnt[lane][dq] = inc - c;
-        if (lane == 31) hist[dq] = inc;
+        hist[tid] = run;
       }
       __syncthreads();
       if (valid) {

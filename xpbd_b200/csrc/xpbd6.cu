@@ -1540,18 +1540,6 @@ static inline size_t bp_fused_smem(int n) {
 // bodies per 8-lane group: ceil(ceil(n / cluster) / 128) <= 16 for n <= 2048
 constexpr int kMaxGroupBodies = 16;
 
-// shared-memory float4 access that the compiler may not cache (refit hand-off)
-XD float4 ld_vol4(const float4* p) {
-  const volatile float* q = reinterpret_cast<const volatile float*>(p);
-  return make_float4(q[0], q[1], q[2], q[3]);
-}
-XD void st_vol4(float4* p, float4 v) {
-  volatile float* q = reinterpret_cast<volatile float*>(p);
-  q[0] = v.x;
-  q[1] = v.y;
-  q[2] = v.z;
-  q[3] = v.w;
-}
 
 __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts, int* status) {
   extern __shared__ __align__(16) unsigned char bp_dyn[];
@@ -1652,12 +1640,16 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
   }
   if (tid == 0) parent[0] = -1;
   __syncthreads();  // the keys are dead: region A now holds the internal bounds
-  // 5. bottom-up refit: the second child to arrive at a node writes its union
+  // 5. bottom-up refit: the second child to arrive at a node writes its union.
+  // Hand-off: the first arriver's union is stored before its fence and flag
+  // atomic; the second arriver reads it after its atomic and fence (fence-fence
+  // synchronisation through the flag; the fences also keep the compiler from
+  // moving the plain shared-memory accesses across them).
   auto node_lo = [&](int x) -> float4 {
-    return x >= n - 1 ? LO[vals[x - (n - 1)]] : ld_vol4(INLO + x);
+    return x >= n - 1 ? LO[vals[x - (n - 1)]] : INLO[x];
   };
   auto node_hi = [&](int x) -> float4 {
-    return x >= n - 1 ? HI[vals[x - (n - 1)]] : ld_vol4(INHI + x);
+    return x >= n - 1 ? HI[vals[x - (n - 1)]] : INHI[x];
   };
   for (int k = tid; k < n; k += T) {
     int cur = parent[n - 1 + k];
@@ -1671,8 +1663,8 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
       __threadfence_block();
       int2 c = child[cur];
       float4 l0 = node_lo(c.x), l1 = node_lo(c.y), h0 = node_hi(c.x), h1 = node_hi(c.y);
-      st_vol4(INLO + cur, make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f));
-      st_vol4(INHI + cur, make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f));
+      INLO[cur] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
+      INHI[cur] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
       cur = parent[cur];
     }
   }
