@@ -1870,24 +1870,19 @@ __global__ void __launch_bounds__(1024) k6_bp_fused(Dev6 s, Par6 p, int* counts,
         });
       }
       __syncwarp();
-      if (live && l == 0) {
-        if (staged) {  // insertion sort by j in shared memory (the partners are distinct)
-          for (int a = 1; a < body_total; ++a) {
-            int key = stage[a], b2 = a - 1;
-            while (b2 >= 0 && stage[b2] > key) {
-              stage[b2 + 1] = stage[b2];
-              --b2;
-            }
-            stage[b2 + 1] = key;
-          }
-        } else {
-          sort_segment(s.pairs, base, min(base + body_total, s.cap));
+      if (live && staged) {
+        // ordered by j without sorting the stage: a partner's slot is the number
+        // of staged partners below it (the partners are distinct), so the lanes
+        // rank and write their partners independently
+        for (int q = l; q < body_total; q += 8) {
+          const int key = stage[q];
+          int rank = 0;
+          for (int a = 0; a < body_total; ++a) rank += stage[a] < key ? 1 : 0;
+          if (base + rank < s.cap) s.pairs[base + rank] = make_int2(i, key);
         }
+      } else if (live && l == 0) {
+        sort_segment(s.pairs, base, min(base + body_total, s.cap));
       }
-      __syncwarp();
-      if (live && staged)
-        for (int q = l; q < body_total; q += 8)
-          if (base + q < s.cap) s.pairs[base + q] = make_int2(i, stage[q]);
       __syncwarp();
     }
   }
