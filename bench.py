@@ -305,7 +305,7 @@ def time_batch(args, device, flush_buf, clocks=None, rank=0, world=1, n_scenes=2
             ach = alg / (kern[name] / 1e3) / 1e9
             rl[name] = {"kernel": "k3_frames (gs, grid)" if name == "cloth" else "LBVH chain + k6_substeps",
                         "alg_bytes_per_frame": int(alg), "ms": round(kern[name], 5), "achieved_gbs": round(ach, 1),
-                        "frac": round(ach / hbm, 4)}
+                        "frac": round(ach / hbm, 4), "traffic": traffic_for(f"batch_{name}")}
     return dict(total_ms=sum(frame_ms), frame_ms=frame_ms, kern_ms=frame_ms, proj_total=proj_total,
                 rows=rows3, bodies=n3 + n6, status=(b.piles.status() if b.has_piles else 0) |
                 (b.cloth.status() if b.has_cloth else 0), alg_bytes=alg3 + alg6,
