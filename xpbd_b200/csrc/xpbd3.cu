@@ -330,6 +330,21 @@ XD void put3(float4* x, int i, V3 p) { x[i] = f4(p, x[i].w); }
 // before projecting any of them.
 XD bool gs_uses_b(int t) { return t == XPBD_DISTANCE || t == XPBD_CONTACT; }
 XD bool gs_uses_xp(int t) { return t == XPBD_FLOOR || t == XPBD_CONTACT; }
+// This CTA's share (part of parts) of elements [lo, hi) of an array, prefetched
+// into L2 with one bulk prefetch (a hint: no data moves to the SM).  The share
+// is rounded inward to 16-byte boundaries, so the range never leaves [lo, hi).
+XD void l2_prefetch_share(const void* base, size_t elem, int lo, int hi, int part, int parts) {
+  const long long n = (long long)hi - lo;
+  if (n <= 0) return;
+  const long long a = lo + n * part / parts, b = lo + n * (part + 1) / parts;
+  unsigned long long s = reinterpret_cast<unsigned long long>(base) + (unsigned long long)a * elem;
+  unsigned long long e = reinterpret_cast<unsigned long long>(base) + (unsigned long long)b * elem;
+  s = (s + 15ull) & ~15ull;
+  e &= ~15ull;
+  if (e > s)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"((unsigned)(e - s)) : "memory");
+}
+
 template <class FGet, class XPGet>
 XD float row_gs_core(float4* x, int4 r, FGet fget, XPGet xpget, const float4* anchor, float lam_old, float h,
                      float4 xa, float4 xb) {
@@ -734,6 +749,13 @@ __global__ void __launch_bounds__(SMEM ? 1024 : 512, 1) k3_frames(Dev3 g, Par3 p
             // endpoints (rows of one color share no particle), then the projections
             for (int c = 0; c < ncol; ++c) {
               const int start = g.cstarts[c], count = g.cstarts[c + 1] - start;
+              if (threadIdx.x == 0) {  // the next colour's packed rows into L2 while this one runs
+                const int cn = c + 1 < ncol ? c + 1 : 0;
+                const int lo = g.cstarts[cn], hi = g.cstarts[cn + 1];
+                l2_prefetch_share(g.gprow, sizeof(int2), lo, hi, (int)blockIdx.x, (int)gridDim.x);
+                l2_prefetch_share(g.gpval, sizeof(float2), lo, hi, (int)blockIdx.x, (int)gridDim.x);
+                l2_prefetch_share(g.glam, sizeof(float), lo, hi, (int)blockIdx.x, (int)gridDim.x);
+              }
               for (int t = tid0; t < count; t += kGsBatch * stride) {
                 int2 pr[kGsBatch];
                 float2 pv[kGsBatch];
