@@ -62,6 +62,12 @@ def make_pile(k, seed):
     return s
 
 
+# Plain Jacobi iterations behind a training target (and behind the previous
+# multiplier a substep carries into the next one's features, in training and
+# in evaluation).
+TARGET_ITERS = 50
+
+
 def generate(n_samples, seed=0, scenes_per_family=200, substeps_per_cloth=8, pile_frames=1, log=print):
     """Alternates cloths and piles until `n_samples`; each scene contributes a
     random subset of at most n_samples / (2 scenes_per_family) of its rows, so
@@ -79,14 +85,14 @@ def generate(n_samples, seed=0, scenes_per_family=200, substeps_per_cloth=8, pil
             s = make_cloth(n, comp)
             for _ in range(int(rng.integers(0, 40))):
                 s.step()
-            f, t = collect(s, substeps=substeps_per_cloth, iters=50)
+            f, t = collect(s, substeps=substeps_per_cloth, iters=TARGET_ITERS)
             kind, what = "cloth", f"cloth {n}x{n} compliance {comp:.2e}"
         else:
             k = int(rng.integers(256, 1441))
             s = make_pile(k, int(rng.integers(1 << 30)))
             for _ in range(int(rng.integers(30, 300))):
                 s.step()
-            f, t = collect6(s, frames=pile_frames, iters=50)
+            f, t = collect6(s, frames=pile_frames, iters=TARGET_ITERS)
             kind, what = "pile", f"pile {s.num_bodies} boxes"
         if len(t) > per_scene:
             sel = torch.randperm(len(t), device=t.device, generator=gen)[:per_scene]
@@ -120,8 +126,8 @@ def evaluate_cloth(m, n=128, compliance=1e-5, frames=30, substeps=16, tol=1e-4, 
     s = make_cloth(n, compliance)
     for _ in range(frames):
         s.step()
-    rows = [iterations_to_tol(s, m, tol=tol, max_iters=max_iters, advance=True, classic=True)
-            for _ in range(substeps)][1:]
+    rows = [iterations_to_tol(s, m, tol=tol, max_iters=max_iters, advance=True, classic=True,
+                              carry_iters=TARGET_ITERS) for _ in range(substeps)][1:]
     plain = np.array([r["plain"] for r in rows])
     learned = np.array([r["learned_with_fallback"] for r in rows])
     classic = np.array([r["classic"] for r in rows])
@@ -142,10 +148,11 @@ def evaluate_cloth(m, n=128, compliance=1e-5, frames=30, substeps=16, tol=1e-4, 
             "plain_final_residual_mean": float(np.mean([r["residual_plain"][-1] for r in rows]))}
 
 
-def evaluate_pile(m, frames_before=240, frames=2, tol=1e-4, max_iters=50, seed=0):
+def evaluate_pile(m, frames_before=240, frames=2, tol=1e-4, max_iters=None, seed=0):
     """The 1440-box pile (12 x 10 x 12, seed 0) after `frames_before` frames; the
     next `frames` frames substep by substep (the first substep of the run has no
     previous converged multiplier and is left out of the means)."""
+    max_iters = TARGET_ITERS if max_iters is None else max_iters
     s = Solver6DOF(device="cuda:0", **PILE_KW)
     scenes.build_box_pile(s, seed=seed)
     for _ in range(frames_before):
@@ -309,10 +316,14 @@ def main():
     ap.add_argument("--out", default=None, help="save the trained weights (float32 .npy)")
     ap.add_argument("--eval", default=None, help="evaluate saved weights instead of training")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--target-iters", type=int, default=50,
+                    help="plain Jacobi iterations behind a target and behind the carried previous multiplier")
     ap.add_argument("--time-infer", type=int, nargs="*", default=None, metavar="ROWS",
                     help="only time the inference launch at these row counts (shipped weights)")
     a = ap.parse_args()
-    report = {}
+    global TARGET_ITERS
+    TARGET_ITERS = a.target_iters
+    report = {"target_iters": TARGET_ITERS}
     if a.time_infer is not None:
         m = WarmStartMLP.pretrained()
         print(json.dumps(time_inference(m, tuple(a.time_infer) or (2400, 14897, 113410, 1 << 20))))
