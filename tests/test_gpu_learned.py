@@ -377,3 +377,32 @@ def test_6dof_warm_start_graph_replay_matches_eager_frames(ws):
     pa, pb = ra.kit.points_total, rb.kit.points_total
     assert pa > 0 and abs(pa - pb) <= 0.02 * pb, (pa, pb)
     assert abs(int(ra.learned_used.item()) - int(rb.learned_used.item())) <= 0.1 * 8 * 15
+
+
+@pytest.mark.parametrize("six", [False, True], ids=["3dof", "6dof"])
+def test_warm_start_that_blows_up_falls_back_to_plain(six):
+    """A network whose output overflows (a huge output bias: lambda0 = inf, so
+    the warm-started first iteration has a non-finite residual) must never be
+    kept: every substep falls back to the plain solve on the device, and the
+    frames stay finite and follow the plain solver's."""
+    bad = WarmStartMLP(seed=5)
+    bad.w[-1] = 1.0e30  # the output bias
+    bad.wb.copy_(bad.w.to(torch.bfloat16))
+    if six:
+        kw = dict(dt=1 / 60, substeps=15, iterations=2, floor_y=0.0, friction=0.6, restitution=0.2)
+        warm, plain = Solver6DOF(warm_start=bad, **kw), Solver6DOF(**kw)
+        for s in (warm, plain):
+            scenes.build_box_pile(s, nx=3, ny=1, nz=3, pitch=1.1, y0=0.5)
+    else:
+        kw = dict(dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi")
+        warm, plain = Solver(warm_start=bad, **kw), Solver(**kw)
+        for s in (warm, plain):
+            scenes.build_cloth(s, res=16, compliance=1e-6)
+    for _ in range(6):
+        warm.step()
+        plain.step()
+    torch.cuda.synchronize()
+    assert int(warm._runner.learned_used.item()) == 0
+    x = warm.positions()
+    assert np.all(np.isfinite(x))
+    np.testing.assert_allclose(x, plain.positions(), atol=1e-4)

@@ -1436,6 +1436,12 @@ extern "C" int xpbd3_launch_info(xpbd3_solver* h, int* blocks, int* threads, int
 // compliant rows |C + alpha~ lambda| (XPBD Eq. 8), reduced to a max per scene.
 // =============================================================================
 namespace xpbd {
+// A row's residual with every non-finite value mapped to +inf, so that a state
+// that blew up never reads as a small residual (a NaN constraint value would
+// otherwise fail the C < 0 test and count as satisfied).
+XD float finite_or_inf(float v) { return v <= 3.402823466e38f ? v : __int_as_float(0x7f800000); }
+XD float hard_violation(float C) { return C < 0.0f ? -C : (C >= 0.0f ? 0.0f : __int_as_float(0x7f800000)); }
+
 __global__ void k3_residual(Dev3 s, float h, const int* row_scene, float* out_scene, float* out_rows) {
   const int m = *s.n_rows;
   const float inv_dt2 = 1.0f / (h * h);
@@ -1450,18 +1456,18 @@ __global__ void k3_residual(Dev3 s, float h, const int* row_scene, float* out_sc
         float wb = r.x == XPBD_ATTACH ? 0.0f : pb.w;
         if (xa.w + wb != 0.0f) {
           float C = length(v3(xa) - v3(pb)) - f.x;
-          res = fabsf(C + (f.y * inv_dt2) * s.lam[j]);
+          res = finite_or_inf(fabsf(C + (f.y * inv_dt2) * s.lam[j]));
         }
       } else if (r.x == XPBD_FLOOR) {
         if (xa.w != 0.0f) {
           float C = xa.y - f.w;
-          res = C < 0.0f ? -C : 0.0f;
+          res = hard_violation(C);
         }
       } else if (r.x == XPBD_CONTACT) {
         float4 xb = s.x[r.z];
         if (xa.w + xb.w != 0.0f) {
           float C = length(v3(xa) - v3(xb)) - f.x;
-          res = C < 0.0f ? -C : 0.0f;
+          res = hard_violation(C);
         }
       }
     }

@@ -2793,7 +2793,12 @@ extern "C" int xpbd6_launch_info(xpbd6_solver* h, int* blocks, int* threads) {
 // the joint's first body, of the floor body, of the incident body).
 // =============================================================================
 namespace xpbd {
-XD void max_into(float* out, int scene, float v) { atomicMax(reinterpret_cast<int*>(out + scene), __float_as_int(v)); }
+// Non-finite values become +inf, so that a state that blew up never reads as a
+// small residual (fmaxf drops a NaN operand, and a NaN compares false).
+XD void max_into(float* out, int scene, float v) {
+  if (!(v <= 3.402823466e38f)) v = __int_as_float(0x7f800000);
+  atomicMax(reinterpret_cast<int*>(out + scene), __float_as_int(v));
+}
 
 __global__ void k6_residual(Dev6 s, Par6 p, const int* body_scene, float* out) {
   const int np = min(*s.n_pairs, s.cap);
@@ -2812,21 +2817,27 @@ __global__ void k6_residual(Dev6 s, Par6 p, const int* body_scene, float* out) {
       if (x4.w == 0.0f) continue;
       V3 he = v3(s.he[i]);
       Q4 qi = q4(s.q[i]);
-      float mx = 0.0f;
-      for (int c = 0; c < 8; ++c) mx = fmaxf(mx, p.floor_y - (v3(x4) + qrot(qi, box_corner(he, c))).y);
-      max_into(out, body_scene ? body_scene[i] : 0, mx);
+      float mx = 0.0f, chk = 0.0f;  // chk: non-finite when any corner is
+      for (int c = 0; c < 8; ++c) {
+        const float v = p.floor_y - (v3(x4) + qrot(qi, box_corner(he, c))).y;
+        mx = fmaxf(mx, v);
+        chk += v * 0.0f;
+      }
+      max_into(out, body_scene ? body_scene[i] : 0, chk == 0.0f ? mx : chk);
     } else {
       int pid = t - s.nj - s.n;
       int4 hdr = s.m_hdr[pid];
       V3 S = v3(s.m_normal[pid]);
-      float mx = 0.0f;
+      float mx = 0.0f, chk = 0.0f;
       for (int c = 0; c < hdr.x; ++c) {
         int slot = 8 * pid + c;
         V3 p_inc = v3(s.x[hdr.y]) + qrot(q4(s.q[hdr.y]), v3(s.m_off_inc[slot]));
         V3 p_ref = v3(s.x[hdr.z]) + qrot(q4(s.q[hdr.z]), v3(s.m_off_ref[slot]));
-        mx = fmaxf(mx, -dot(p_inc - p_ref, S));
+        const float v = -dot(p_inc - p_ref, S);
+        mx = fmaxf(mx, v);
+        chk += v * 0.0f;
       }
-      if (hdr.x) max_into(out, body_scene ? body_scene[hdr.y] : 0, mx);
+      if (hdr.x) max_into(out, body_scene ? body_scene[hdr.y] : 0, chk == 0.0f ? mx : chk);
     }
   }
 }

@@ -191,24 +191,33 @@ class SubstepKit:
         return torch.sign(lam * self.weff) * torch.log1p(torch.abs(lam * self.weff) / LEN)
 
 
-def collect(s, substeps, iters=50, every=1):
+def collect(s, substeps, iters=50, every=1, carry="target"):
     """Generate (features, target) pairs from the plain solver: each substep
     integrates, records the features, solves with `iters` plain Jacobi
-    iterations from lambda = 0, records the target from the converged lambda,
-    and finalizes (so the scene keeps evolving).  Returns concatenated tensors
-    of the rows the warm start acts on."""
+    iterations from lambda = 0 and records the target from that lambda.  With
+    carry="target" the scene then finalizes from that solve, so the target is
+    also the next substep's previous multiplier (feature 3); with carry="run"
+    the solve is undone and the substep runs the solver's own iteration count
+    (as ``step()`` does), whose multipliers become the previous ones.  Returns
+    concatenated tensors of the rows the warm start acts on."""
     kit = SubstepKit(s)
     F, T = [], []
+    X = s.tensors["x"]
     m = int(s.tensors["n_rows"].item())
     for k in range(substeps):
         kit.integrate()
         kit.features()
+        x0 = X.clone() if carry == "run" else None
         for it in range(iters):
             kit.iterate(first=(it == 0))
         if k % every == 0:
             live = kit.weff[:m] > 0
             F.append(kit.feats[:m][live].clone())
             T.append(kit.targets_from(s.tensors["lam"][:m])[live].clone())
+        if x0 is not None:
+            X.copy_(x0)
+            for it in range(s.iterations):
+                kit.iterate(first=(it == 0))
         kit.finalize()
     return torch.cat(F), torch.cat(T)
 
@@ -332,7 +341,9 @@ class WarmStartRunner:
             kit.warm(self.model)
         kit.iterate(first=False)
         self._residual(self.res_l)
-        use_plain = self.res_p <= self.res_l
+        # plain unless the warm start's residual is strictly smaller (ties and a
+        # non-finite warm-started residual keep the plain solve)
+        use_plain = ~(self.res_l < self.res_p)
         T["x"].copy_(torch.where(use_plain, self.x_plain, T["x"]))
         T["lam"].copy_(torch.where(use_plain, self.lam_plain, T["lam"]))
         self.learned_used += (~use_plain).to(torch.int32)
@@ -552,13 +563,14 @@ class SubstepKit6:
         self.finish()
 
 
-def collect6(s, frames, iters=50, floor_gap=0.01):
+def collect6(s, frames, iters=50, floor_gap=0.01, carry="target"):
     """(features, target) pairs from the plain solver on a box scene: the scene
     advances with its normal iteration count; at every substep the target is
     the multiplier after `iters` plain iterations from the same post-integrate
-    state, and that multiplier is the next substep's previous multiplier
-    (feature 3).  Floor slots are kept when the corner is within
-    `floor_gap` of the floor or its target is non-zero."""
+    state, and (carry="target") that multiplier is the next substep's previous
+    multiplier (feature 3), or (carry="run") the multiplier of the scene's own
+    iterations is, as in ``step()``.  Floor slots are kept when the corner is
+    within `floor_gap` of the floor or its target is non-zero."""
     kit = SubstepKit6(s)
     F, T = [], []
     gap = float(np.log1p(floor_gap / LEN))
@@ -571,7 +583,8 @@ def collect6(s, frames, iters=50, floor_gap=0.01):
                 kit.iterate()
             lam = kit.lam_rows()
             tgt = kit.targets_from(lam)
-            kit.carry(lam)
+            if carry == "target":
+                kit.carry(lam)
             keep = kit.weff > 0
             keep[: kit.nf] &= (kit.feats[: kit.nf, 0] < gap) | (tgt[: kit.nf] != 0)
             F.append(kit.feats[keep].clone())
@@ -583,27 +596,33 @@ def collect6(s, frames, iters=50, floor_gap=0.01):
     return torch.cat(F), torch.cat(T)
 
 
-def iterations_to_tol6(kit, model=None, tol=1e-4, max_iters=50, scale=1.0, variants=None):
+def iterations_to_tol6(kit, model=None, tol=1e-4, max_iters=50, scale=1.0, variants=None, carry_iters=None):
     """One substep of a box scene from its current state: the residual after
     every Jacobi iteration of the plain solve (lambda0 = 0) and of the
     warm-started solve, the iterations each needs to reach `tol` (max_iters + 1
     if never) and to reach the plain solve's final residual, and the
     per-substep fallback (plain kept when the learned first iteration is worse).
     The scene then completes the substep with its normal iterations, and the
-    plain solve's `max_iters`-iteration multipliers become the next substep's
-    previous multipliers (as in ``collect6``)."""
+    plain solve's multipliers after `carry_iters` iterations (default
+    `max_iters`) become the next substep's previous multipliers (as in
+    ``collect6``)."""
     s = kit.s
     kit.begin()
     snap = kit.snapshot()
+
+    carry_at = max_iters if carry_iters is None else min(carry_iters, max_iters)
+    carried = {}
 
     def run(use_model, sc=scale, lam0=None):
         kit.restore(snap)
         if use_model or lam0 is not None:
             kit.warm(model, sc, lam0)
         res = []
-        for _ in range(max_iters):
+        for k in range(max_iters):
             kit.iterate()
             res.append(kit.residual())
+            if k + 1 == carry_at and not (use_model or lam0 is not None):
+                carried["plain"] = kit.lam_rows().clone()
         return res
 
     def first_below(res, t):
@@ -612,7 +631,7 @@ def iterations_to_tol6(kit, model=None, tol=1e-4, max_iters=50, scale=1.0, varia
 
     out = {}
     rp = run(False)
-    lam_plain = kit.lam_rows().clone()
+    lam_plain = carried["plain"]
     out["plain"] = first_below(rp, tol)
     out["residual_plain"] = rp
     if model is not None:
@@ -685,7 +704,9 @@ class WarmStartRunner6:
             kit.warm(self.model)
         kit.iterate()
         self._residual(self.res_l)
-        use_plain = self.res_p <= self.res_l
+        # plain unless the warm start's residual is strictly smaller (ties and a
+        # non-finite warm-started residual keep the plain solve)
+        use_plain = ~(self.res_l < self.res_p)
         for cur, p in zip((T["x"], T["q"], T["lam_floor"], T["lam_pair"], kit.tot_floor), plain):
             cur.copy_(torch.where(use_plain, p, cur))
         self.learned_used += (~use_plain).to(torch.int32)

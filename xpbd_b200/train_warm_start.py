@@ -66,6 +66,10 @@ def make_pile(k, seed):
 # multiplier a substep carries into the next one's features, in training and
 # in evaluation).
 TARGET_ITERS = 50
+# Which multiplier a substep carries into the next one's features: "target"
+# (the TARGET_ITERS-iteration solve's) or "run" (the solver's own iterations',
+# as step() carries it).
+CARRY = "target"
 
 
 def generate(n_samples, seed=0, scenes_per_family=200, substeps_per_cloth=8, pile_frames=1, log=print):
@@ -85,14 +89,14 @@ def generate(n_samples, seed=0, scenes_per_family=200, substeps_per_cloth=8, pil
             s = make_cloth(n, comp)
             for _ in range(int(rng.integers(0, 40))):
                 s.step()
-            f, t = collect(s, substeps=substeps_per_cloth, iters=TARGET_ITERS)
+            f, t = collect(s, substeps=substeps_per_cloth, iters=TARGET_ITERS, carry=CARRY)
             kind, what = "cloth", f"cloth {n}x{n} compliance {comp:.2e}"
         else:
             k = int(rng.integers(256, 1441))
             s = make_pile(k, int(rng.integers(1 << 30)))
             for _ in range(int(rng.integers(30, 300))):
                 s.step()
-            f, t = collect6(s, frames=pile_frames, iters=TARGET_ITERS)
+            f, t = collect6(s, frames=pile_frames, iters=TARGET_ITERS, carry=CARRY)
             kind, what = "pile", f"pile {s.num_bodies} boxes"
         if len(t) > per_scene:
             sel = torch.randperm(len(t), device=t.device, generator=gen)[:per_scene]
@@ -126,8 +130,9 @@ def evaluate_cloth(m, n=128, compliance=1e-5, frames=30, substeps=16, tol=1e-4, 
     s = make_cloth(n, compliance)
     for _ in range(frames):
         s.step()
+    carry_iters = TARGET_ITERS if CARRY == "target" else s.iterations
     rows = [iterations_to_tol(s, m, tol=tol, max_iters=max_iters, advance=True, classic=True,
-                              carry_iters=TARGET_ITERS) for _ in range(substeps)][1:]
+                              carry_iters=carry_iters) for _ in range(substeps)][1:]
     plain = np.array([r["plain"] for r in rows])
     learned = np.array([r["learned_with_fallback"] for r in rows])
     classic = np.array([r["classic"] for r in rows])
@@ -163,7 +168,8 @@ def evaluate_pile(m, frames_before=240, frames=2, tol=1e-4, max_iters=None, seed
     for f in range(frames):
         kit.broadphase()
         for _ in range(s.substeps):
-            rows.append(iterations_to_tol6(kit, m, tol=tol, max_iters=max_iters, variants=prev))
+            rows.append(iterations_to_tol6(kit, m, tol=tol, max_iters=max_iters, variants=prev,
+                                           carry_iters=None if CARRY == "target" else s.iterations))
     rows = rows[1:]
     pf_plain = np.array([r["to_plain_final"]["plain"] for r in rows])
     pf_learn = np.array([r["to_plain_final"]["learned"] for r in rows])
@@ -318,12 +324,16 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--target-iters", type=int, default=50,
                     help="plain Jacobi iterations behind a target and behind the carried previous multiplier")
+    ap.add_argument("--carry", choices=["target", "run"], default="target",
+                    help="the multiplier a substep carries into the next one's features: the target solve's, "
+                         "or the solver's own iterations' (as step())")
     ap.add_argument("--time-infer", type=int, nargs="*", default=None, metavar="ROWS",
                     help="only time the inference launch at these row counts (shipped weights)")
     a = ap.parse_args()
-    global TARGET_ITERS
+    global TARGET_ITERS, CARRY
     TARGET_ITERS = a.target_iters
-    report = {"target_iters": TARGET_ITERS}
+    CARRY = a.carry
+    report = {"target_iters": TARGET_ITERS, "carry": CARRY}
     if a.time_infer is not None:
         m = WarmStartMLP.pretrained()
         print(json.dumps(time_inference(m, tuple(a.time_infer) or (2400, 14897, 113410, 1 << 20))))
