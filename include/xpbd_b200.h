@@ -223,11 +223,15 @@ int xpbd3_features(const xpbd3_state* s, float h, float gx, float gy, float gz, 
  * are rounded to bf16.  feats: m x 8 floats (7 used). */
 int xpbd_mlp_infer(const float* feats, const float* weff, int m, const void* weights_bf16, float* lam0,
                    void* stream);
-/* 1 in *status if an inference launch gave up waiting for the tensor core
- * (bounded wait; that launch wrote its remaining rows as NaN), else 0;
- * reset != 0 clears it.  Synchronous. */
+/* 1 in *status if an inference or gradient launch gave up waiting for the
+ * tensor core (bounded wait; an inference launch writes its remaining rows as
+ * NaN, a gradient launch adds NaN to the loss), else 0; reset != 0 clears it.
+ * Synchronous. */
 int xpbd_mlp_status(int* status, int reset);
-/* Loss (mean squared error) of a batch and its gradient, added into G. */
+/* Loss (mean squared error) of a batch and its gradient, added into G.  The
+ * forward, input-gradient and weight-gradient products run on the tensor cores
+ * (tcgen05, 128-sample tiles, bf16 operands: the first layer's activations and
+ * dL/dz2 are rounded to bf16). */
 int xpbd_mlp_grads(const float* feats, const float* targets, int B, const void* weights_bf16, float* G,
                    float* loss, void* stream);
 /* One Adam step on fp32 master weights w (moments M, V); refreshes the bf16 copy, clears G. */
