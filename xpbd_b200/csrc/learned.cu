@@ -237,6 +237,9 @@ __global__ void __launch_bounds__(256) k_mlp_infer_tc(const float* feats, const 
 // At the end every CTA adds its gradient into G (one atomic per weight) and its
 // loss share into `loss`.
 constexpr int kT = 128;
+// Row stride (floats) of the [sample][unit] tile: one more than the 64 units,
+// so the 32 samples of a warp writing the same unit hit 32 different banks.
+constexpr int kFStride = kHid + 1;
 // Byte offset of element (row, k) of a K-major operand of 128 columns (K = 128).
 XD uint32_t kmajor128_off(int row, int k) {
   return (uint32_t)((row >> 3) * 2048 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
@@ -250,8 +253,8 @@ struct GradSmem {  // byte offsets into the dynamic shared memory (base aligned 
   static constexpr uint32_t A1T = DZ2T + 32768;      // [k][s] bf16, K = 128
   static constexpr uint32_t W2 = A1T + 16384;        // [u][k] bf16
   static constexpr uint32_t W2T = W2 + 8192;         // [k][u] bf16
-  static constexpr uint32_t F = W2T + 8192;          // fp32 [s][64]: dy a2, then dz1
-  static constexpr uint32_t GACC = F + 32768;        // fp32 [kNParam] (the W2 block unused)
+  static constexpr uint32_t F = W2T + 8192;          // fp32 [s][kFStride]: dy a2, then dz1
+  static constexpr uint32_t GACC = F + 4 * kT * kFStride;  // fp32 [kNParam] (the W2 block unused)
   static constexpr uint32_t WF = GACC + 4 * 4740;    // fp32 W1 (448), b1, b2, W3 (64 each)
   static constexpr uint32_t X = WF + 4 * 640;        // fp32 [s][8]
   static constexpr uint32_t TGT = X + 4 * kT * 8;    // fp32 [s]
@@ -398,7 +401,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grads_tc(const float* feats, con
         for (int e2 = 0; e2 < 2; ++e2) {
           const int i = 8 * c + 2 * q + e2, u = 32 * h + i;
           d[e2] = bf16r(dy * sW3[u] * gelu_d(z2[i]));
-          sF[r * kHid + u] = dy * a2[i];
+          sF[r * kFStride + u] = dy * a2[i];
           *reinterpret_cast<__nv_bfloat16*>(sm + S::DZ2T + kmajor128_off(u, r)) = d[e2];
         }
         __nv_bfloat162 p2;
@@ -428,7 +431,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grads_tc(const float* feats, con
     // the tile's sums for W3, b2, b3 while the tensor core works
     if (t < kHid) {
       float acc = 0.0f;
-      for (int s = 0; s < kT; ++s) acc += sF[s * kHid + t];
+      for (int s = 0; s < kT; ++s) acc += sF[s * kFStride + t];
       gacc[oW3 + t] += acc;
     } else if (t < 2 * kHid) {
       const int u = t - kHid;
@@ -454,7 +457,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grads_tc(const float* feats, con
         float z = sB1[u];
 #pragma unroll
         for (int k = 0; k < kIn; ++k) z = __fmaf_rn(sW1[u * kIn + k], x[k], z);
-        sF[r * kHid + u] = da1[i] * gelu_d(z);
+        sF[r * kFStride + u] = da1[i] * gelu_d(z);
       }
     }
     tc::fence_before_sync();
@@ -464,11 +467,11 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grads_tc(const float* feats, con
       float acc = 0.0f;
       if (o < kHid * kIn) {
         const int u = o / kIn, k = o % kIn;
-        for (int s = 0; s < kT; ++s) acc = __fmaf_rn(sF[s * kHid + u], sX[s * 8 + k], acc);
+        for (int s = 0; s < kT; ++s) acc = __fmaf_rn(sF[s * kFStride + u], sX[s * 8 + k], acc);
         gacc[oW1 + o] += acc;
       } else {
         const int u = o - kHid * kIn;
-        for (int s = 0; s < kT; ++s) acc += sF[s * kHid + u];
+        for (int s = 0; s < kT; ++s) acc += sF[s * kFStride + u];
         gacc[oB1 + u] += acc;
       }
     }

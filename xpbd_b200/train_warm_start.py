@@ -3,6 +3,7 @@
     python -m xpbd_b200.train_warm_start --samples 10000000 --out weights.npy
     python -m xpbd_b200.train_warm_start --eval weights.npy
     python -m xpbd_b200.train_warm_start --time-infer [ROWS ...]
+    python -m xpbd_b200.train_warm_start --time-grads [SAMPLES ...]
 
 Data (half from each family, by sample count):
   * randomized cloths (n x n, n ~ U{32..128}; spacing 0.02 m, 0.01 kg, two
@@ -218,6 +219,29 @@ def time_inference(m, rows_list=(2400, 14897, 113410, 1 << 20), reps=50, seed=0)
     return out
 
 
+def time_gradient(m, batches=(65536, 1 << 20), reps=20, seed=0):
+    """Device time of one ``xpbd_mlp_grads`` launch (tensor-core training
+    kernel) per batch size, on random features and targets (mean of `reps`
+    launches, CUDA events)."""
+    from . import _native as N
+    rng = np.random.default_rng(seed)
+    out = {}
+    for B in batches:
+        feats = torch.from_numpy(rng.normal(size=(B, 8)).astype(np.float32)).cuda()
+        targets = torch.from_numpy(rng.normal(size=B).astype(np.float32)).cuda()
+        loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+
+        def run():
+            N.check(m.F["grads"](N.ptr(feats), N.ptr(targets), B, N.ptr(m.wb), N.ptr(m.G), N.ptr(loss),
+                                 N.stream_of("cuda:0")), "xpbd_mlp_grads")
+        us = _event_ms(run, reps=reps) * 1e3
+        if not bool(torch.isfinite(m.G).all()):
+            raise RuntimeError("non-finite gradient")
+        m.G.zero_()
+        out[str(B)] = {"us": round(us, 1), "samples_per_s": round(B / (us * 1e-6), 1)}
+    return out
+
+
 def time_warm_start(m):
     """Device time of the warm start's extra work per substep (features +
     inference + warm apply) against one plain Jacobi iteration (solve + apply),
@@ -329,6 +353,8 @@ def main():
                          "or the solver's own iterations' (as step())")
     ap.add_argument("--time-infer", type=int, nargs="*", default=None, metavar="ROWS",
                     help="only time the inference launch at these row counts (shipped weights)")
+    ap.add_argument("--time-grads", type=int, nargs="*", default=None, metavar="SAMPLES",
+                    help="only time the gradient launch at these batch sizes (shipped weights)")
     a = ap.parse_args()
     global TARGET_ITERS, CARRY
     TARGET_ITERS = a.target_iters
@@ -337,6 +363,10 @@ def main():
     if a.time_infer is not None:
         m = WarmStartMLP.pretrained()
         print(json.dumps(time_inference(m, tuple(a.time_infer) or (2400, 14897, 113410, 1 << 20))))
+        return
+    if a.time_grads is not None:
+        m = WarmStartMLP.pretrained()
+        print(json.dumps(time_gradient(m, tuple(a.time_grads) or (65536, 1 << 20))))
         return
     if a.eval:
         m = WarmStartMLP()
