@@ -486,11 +486,12 @@ def time_engine6(args, workload, device, world, flush_buf, clocks=None):
 
 def time_e2e(args, workload, device):
     """Same metric through the public API with host buffers.  Every frame: the
-    state (3-DOF: x, v; 6-DOF: x, q, v, w) is uploaded from pinned host memory,
-    ``step()`` runs, and the state (plus the live row count, 3-DOF) is read back
-    into pinned host memory, which feeds the next frame; the stream is
-    synchronised each frame.  The region is bracketed by CUDA events on the
-    solver's stream."""
+    state (3-DOF: x, v; 6-DOF: x, q, v, w -- the solver keeps them as the rows
+    of one contiguous block, ``tensors["state"]``, so one copy each way) is
+    uploaded from pinned host memory, ``step()`` runs, and the state (plus the
+    live row count, 3-DOF) is read back into pinned host memory, which feeds
+    the next frame; the stream is synchronised each frame.  The region is
+    bracketed by CUDA events on the solver's stream."""
     import torch
 
     from xpbd_b200 import Solver, Solver6DOF
@@ -502,7 +503,7 @@ def time_e2e(args, workload, device):
         s.sync_contacts = False
     s._flush()
     T = s.tensors
-    keys = ("x", "q", "v", "w") if six else ("x", "v")
+    keys = ("state",)
     host = {k: T[k].cpu().pin_memory() for k in keys}
     rows_host = torch.zeros(args.steps, dtype=torch.int32).pin_memory()
     stream = torch.cuda.current_stream(device)

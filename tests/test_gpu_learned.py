@@ -381,12 +381,14 @@ def test_6dof_warm_start_graph_replay_matches_eager_frames(ws):
 
 @pytest.mark.parametrize("six", [False, True], ids=["3dof", "6dof"])
 def test_warm_start_that_blows_up_falls_back_to_plain(six):
-    """A network whose output overflows (a huge output bias: lambda0 = inf, so
-    the warm-started first iteration has a non-finite residual) must never be
-    kept: every substep falls back to the plain solve on the device, and the
+    """A network whose prediction is absurd but finite (an output bias of 80 in
+    the log units: lambda0 near 1e31 on every row, which the warm-start kernels
+    apply, unlike a non-finite lambda0, which they drop) must never be kept:
+    the warm-started first iteration leaves an enormous or non-finite residual,
+    so every substep falls back to the plain solve on the device, and the
     frames stay finite and follow the plain solver's."""
     bad = WarmStartMLP(seed=5)
-    bad.w[-1] = 1.0e30  # the output bias
+    bad.w[-1] = 80.0  # the output bias
     bad.wb.copy_(bad.w.to(torch.bfloat16))
     if six:
         kw = dict(dt=1 / 60, substeps=15, iterations=2, floor_y=0.0, friction=0.6, restitution=0.2)

@@ -228,8 +228,10 @@ class Solver:
             row_f[:ms, 3] = an[:, 1]
             row_a[:ms, :3] = an
         T = {}
-        T["x"] = torch.from_numpy(x).to(dev)
-        T["v"] = torch.from_numpy(v).to(dev)
+        # x and v are the two rows of one contiguous block (`state`), so a caller
+        # moving the state to or from the host needs one copy each way
+        T["state"] = torch.from_numpy(np.stack([x, v])).to(dev)
+        T["x"], T["v"] = T["state"].unbind(0)
         T["x_prev"] = torch.zeros((n, 4), dtype=torch.float32, device=dev)
         T["acc"] = torch.zeros((n, 4), dtype=torch.float32, device=dev)
         T["row_i"] = torch.from_numpy(row_i).to(dev)

@@ -258,10 +258,14 @@ class Solver6DOF:
                     raise IndexError(f"{nm} references a body outside [0, {n})")
         T = {}
         self._t = T
-        T["x"] = f4(x, self._inv_mass)
-        T["q"] = torch.from_numpy(q.copy()).to(dev)
-        T["v"] = f4(v)
-        T["w"] = f4(w)
+        # x, q, v, w are the four rows of one contiguous block (`state`), so a
+        # caller moving the state to or from the host needs one copy each way
+        T["state"] = torch.empty((4, n, 4), dtype=torch.float32, device=dev)
+        T["state"][0].copy_(f4(x, self._inv_mass))
+        T["state"][1].copy_(torch.from_numpy(q.copy()).to(dev))
+        T["state"][2].copy_(f4(v))
+        T["state"][3].copy_(f4(w))
+        T["x"], T["q"], T["v"], T["w"] = T["state"].unbind(0)
         T["x_prev"] = torch.zeros((n, 4), dtype=torch.float32, device=dev)
         T["q_prev"] = torch.zeros((n, 4), dtype=torch.float32, device=dev)
         T["inv_I"] = f4(self._inv_I)
