@@ -101,3 +101,22 @@ def test_pile_residual_statistics_over_seeds(name):
                     orc_all.append(r_orc)
     ratio = float(np.mean(eng_all) / np.mean(orc_all))
     assert abs(ratio - 1.0) <= STAT_BOUND[name], ratio
+
+
+@pytest.mark.parametrize("six", [False, True], ids=["3dof", "6dof"])
+def test_residual_reports_a_non_finite_state_as_infinite(six):
+    """A state that blew up (one body's position NaN) must not read as a small
+    residual: a NaN constraint value fails the hard rows' C < 0 test and a
+    maximum with fmaxf drops NaN operands, so the residual kernels map every
+    non-finite row to +inf.  The warm-start fallback relies on it."""
+    if six:
+        s = Solver6DOF(device="cuda:0", dt=1 / 60, substeps=15, iterations=2, floor_y=0.0)
+        scenes.build_box_pile(s, nx=3, ny=2, nz=3)
+    else:
+        s = Solver(device="cuda:0", dt=1 / 60, substeps=15, iterations=2, solve_mode="jacobi")
+        scenes.build_cloth(s, res=8)
+    s.step()
+    assert np.all(np.isfinite(s.residual()))
+    s.tensors["x"][2, 1] = float("nan")
+    r = s.residual()
+    assert np.isinf(r[0]) and r[0] > 0, r
